@@ -1,0 +1,372 @@
+"""Benchmark of the B200 QuickPIC slice engine (one JSON line on rank 0).
+
+Workload (default, --config medium): the 512 x 512 x 512 plain-method case --
+transverse grid 512^2 over 12 x 12 c/wp, 512 slices over 10 c/wp, uniform
+plasma with 2 x 2 particles per cell (the reference loader gives
+510 * 511 * 4 = 1,042,440 FP32 electrons), tri-Gaussian drive beam of
+256 x 256 x 128 = 8,388,608 macro-particles, sigma_r = 0.3, sigma_z = 0.6 c/wp,
+nb/np = 4, gamma = 20000 with 1% energy spread and normalised emittance 0.01.
+A step is one 3D step: beam deposit, all 512 slices, species renew.
+Inputs are synthetic (seeded loaders of the reference, no dataset).
+
+metric: plasma particle-slices/s = (plasma particles x slices) / device time.
+value  = inputs resident on the GPU; e2e = the same through the public API with
+the beam particles copied from pinned host memory each step and the on-axis
+wake lineout read back.
+
+--impl reference: the reference's algorithm on the host cores (the CPU oracle,
+QuickPIC's routines restated in C++/OpenMP; the Fortran reference needs gfortran,
+MPI, HDF5 and json-fortran, none of which exist in this image), timed on a
+bounded sample of slices of the same workload.
+Multi-GPU: the path does not shard (slices are a recurrence in xi); --gpus N
+runs N independent replicas, one per GPU, and value is their aggregate.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "quickpic-opensource_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+BOX = [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]]
+
+CONFIGS = {
+    # the plain-method medium case (512^3, 4 ppc, 8.4M beam particles)
+    "medium": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2,
+                   species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                   beams=[dict(np=[256, 256, 128], q=-1.0, m=1.0, gamma=20000.0,
+                               peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
+                               sigma=[0.3, 0.3, 0.6],
+                               sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the small CPU-runnable case (128^3, 2x2 ppc, 262,144 beam particles)
+    "small": dict(grid=dict(ind=[7, 7, 7], box=BOX), iter=2,
+                  species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                  beams=[dict(np=[64, 64, 64], q=-1.0, m=1.0, gamma=20000.0,
+                              peak_density=2.0, quiet_start=True, center=[0.0, 0.0, 2.5],
+                              sigma=[0.3, 0.3, 0.5], sigma_v=[0.0, 0.0, 0.0])]),
+}
+
+
+def plasma_count(cfg):
+    nx, ny = (1 << cfg["grid"]["ind"][0]), (1 << cfg["grid"]["ind"][1])
+    ppc = cfg["species"]["ppc"]
+    return (nx - 2) * (ny - 1) * ppc[0] * ppc[1]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in a thread."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
+        if f.get("kernel") == kernel and f.get("workload") == workload:
+            return float(f["dram_bytes_per_launch"])
+    return None
+
+
+def make_engine(qpgpu, cfg, device):
+    g = cfg["grid"]
+    ctx = qpgpu.Context(g["ind"][0], g["ind"][1], g["ind"][2], g["box"], device=device)
+    s = cfg["species"]
+    sp = qpgpu.Species2d(ctx, ppc=tuple(s["ppc"]), q=s["q"], m=s["m"], density=s["density"],
+                         xtras=s["xtras"])
+    beams = []
+    for b in cfg["beams"]:
+        beams.append(qpgpu.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
+                                  peak_density=b["peak_density"], quiet_start=b["quiet_start"],
+                                  center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
+    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=True)
+    return ctx, sp, beams, sim
+
+
+def run_engine(args, cfg, rank, world, local_rank, dist):
+    import qpgpu
+
+    ctx, sp, beams, sim = make_engine(qpgpu, cfg, local_rank)
+    npl = sp.np()
+    nz = ctx.nz
+    for _ in range(args.warmup):
+        st = sim.step3d()
+    kernels_per_step = st.kernels if args.warmup else 0
+
+    def barrier():
+        ctx.sync()
+        if dist is not None:
+            import torch
+
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    # ---- value: inputs resident in HBM
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    ctx.timer_start()
+    regrow = 0
+    for _ in range(args.steps):
+        st = sim.step3d()
+        regrow += st.regrowths
+        kernels_per_step = st.kernels
+    t_ms = ctx.timer_stop()
+    clocks.stop()
+    barrier()
+    t_ms = max_over_ranks(t_ms, dist)
+    value = npl * nz * args.steps * world / (t_ms * 1e-3)
+
+    # ---- e2e: beam in from pinned host memory, wake lineout out, every step
+    import torch
+
+    bm = beams[0]
+    host = bm.get_particles()
+    pinned = torch.empty(host.size, dtype=torch.float32, pin_memory=True).numpy()
+    pin2 = pinned.reshape(host.shape, order="F")
+    pin2[...] = host
+    line = torch.empty(nz + 1, dtype=torch.float32, pin_memory=True).numpy()
+    barrier()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        bm.set_particles(pin2)
+        sim.step3d()
+        sim.lineout(3, out=line)
+    e_ms = ctx.timer_stop()
+    barrier()
+    e_ms = max_over_ranks(e_ms, dist)
+    e2e = {"value": npl * nz * args.steps * world / (e_ms * 1e-3), "unit": "particle-slices/s",
+           "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(line.nbytes),
+           "ms_per_step": e_ms / args.steps}
+
+    # ---- roofline of the dominant kernel, from a per-launch profile of 16 slices
+    prof = sim.profile(min(16, nz))
+    peak, peak_kind = load_peaks()
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    name, (ms, cnt, byts) = top
+    tot = sum(v[0] for v in prof.values())
+    achieved = (byts / cnt) / (ms / cnt * 1e-3) / 1e9 if ms > 0 else 0.0
+    traffic = ncu_traffic(name, args.config)
+    roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": peak_kind, "share": round(ms / tot, 4),
+                "algorithmic_bytes_per_launch": byts / cnt,
+                "avg_launch_us": round(ms / cnt * 1e3, 2)}
+    kernels = {k: {"ms": round(v[0], 4), "launches": v[1],
+                   "GBps": round(v[2] / (v[0] * 1e-3) / 1e9, 1) if v[0] > 0 and v[2] > 0 else None}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    sim.close()
+    for b in beams:
+        b.close()
+    sp.close()
+    ctx.close()
+    return dict(value=value, t_ms=t_ms, e2e=e2e, roofline=roofline, kernels=kernels,
+                clocks=clocks.summary(), npl=npl, nz=nz, regrow=regrow,
+                launches=kernels_per_step * args.steps,
+                beam_np=int(sum(np.prod(b["np"]) for b in cfg["beams"])))
+
+
+def max_over_ranks(v, dist):
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_slices(cfg, budget_s, max_slices, threads):
+    """Time slices of the oracle (the reference's routines restated, FP32, OpenMP).
+
+    Returns (particle-slices/s, slices timed, seconds, plasma particles)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    c = dict(cfg)
+    c["store3d"] = False
+    sim = oracle.Sim(c, np.float32)
+    sim.begin3d()
+    npl = int(sim.get("np")[0])
+    t0 = time.perf_counter()
+    j = 0
+    while j < max_slices:
+        j += 1
+        sim.slice(j)
+        if time.perf_counter() - t0 >= budget_s and j >= 2:
+            break
+    dt = time.perf_counter() - t0
+    sim.close()
+    return npl * j / dt, j, dt, npl
+
+
+def workload_desc(cfg, name):
+    g = cfg["grid"]["ind"]
+    b = cfg["beams"][0]
+    return (f"{name}: {1 << g[0]}x{1 << g[1]} transverse, {1 << g[2]} slices, "
+            f"{cfg['species']['ppc'][0]}x{cfg['species']['ppc'][1]} ppc, beam "
+            f"{int(np.prod(b['np']))} particles sigma_r={b['sigma'][0]} sigma_z={b['sigma'][2]} "
+            f"nb/np={b['peak_density']}, iter={cfg['iter']} (fixed predictor-corrector passes)")
+
+
+def run_reference(args, cfg):
+    threads = os.cpu_count() or 1
+    npl = plasma_count(cfg)
+    per_step = max(2, args.ref_slices)
+    # each step: a bounded sample of `per_step` slices of the same 3D step
+    for _ in range(args.warmup):
+        cpu_slices(cfg, 0.0, 2, threads)
+    vals, secs, nsl = [], 0.0, 0
+    for _ in range(args.steps):
+        v, j, dt, npl = cpu_slices(cfg, 1e9, per_step, threads)
+        vals.append(v)
+        secs += dt
+        nsl += j
+    value = npl * nsl / secs
+    line = {"impl": "reference", "metric": "plasma particle-slices/s", "value": value,
+            "unit": "particle-slices/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded reference loaders)",
+            "config": {"workload": workload_desc(cfg, args.config), "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": "particle-slices/s", "cores": threads,
+                             "kind": "port",
+                             "sample": f"{per_step} slices per step of the {args.config} 3D step "
+                                       f"(CPU restatement of the reference algorithm, FP32, "
+                                       f"OpenMP; not the Fortran binary)"},
+            "e2e": {"value": value, "unit": "particle-slices/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--config", default="medium", choices=sorted(CONFIGS))
+    ap.add_argument("--ref-slices", type=int, default=4)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    r = run_engine(args, cfg, rank, world, local_rank, dist)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, j, dt, npl = cpu_slices(cfg, args.cpu_budget, 64, threads)
+        cpu = {"value": v, "unit": "particle-slices/s", "cores": threads, "kind": "port",
+               "sample": f"first {j} slices of one {args.config} 3D step in {dt:.1f} s "
+                         f"(CPU restatement of the reference algorithm, FP32, OpenMP)"}
+    if rank == 0:
+        line = {"metric": "plasma particle-slices/s", "value": r["value"],
+                "unit": "particle-slices/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["t_ms"] / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded reference loaders)",
+                "config": {"workload": workload_desc(cfg, args.config),
+                           "plasma_particles": r["npl"], "beam_particles": r["beam_np"],
+                           "slices": r["nz"], "iter": cfg["iter"],
+                           "l2": "inputs larger than L2: each 3D step writes >4 GB of 3D fields",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "step_time_ms": r["t_ms"] / args.steps,
+                "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": cpu,
+                "gpu_launches": r["launches"], "clocks": r["clocks"],
+                "regrowths": r["regrow"], "kernels": r["kernels"]}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+/*
+ * qpgpu.h -- C ABI of the B200 engine for QuickPIC's per-slice quasi-static path.
+ *
+ * The engine replaces, behind QuickPIC's own Fortran class API, the plasma
+ * push and deposits (species2d / part2d), the 2D sine/cosine Poisson and B
+ * solves (field2d / fpois2d / fft2d) and the beam 3D deposit (beam3d / part3d)
+ * on one GPU.  A Fortran caller binds these entry points with iso_c_binding
+ * (the binding module is shown in INTEGRATION.md); every argument is a plain
+ * pointer, integer or float, and no call retains a host pointer after it
+ * returns.  Each function below names the reference routine it replaces
+ * (paths relative to QuickPIC-OpenSource/source).
+ *
+ * Conventions
+ *  - Every call returns int: 0 = success; > 0 = recoverable capacity
+ *    overflow (the required capacity is in qp_ctx_last_need(), the caller
+ *    grows and retries, as part2d%pmove does, part2d_class.f03:429-579);
+ *    < 0 = fatal error (message in qp_ctx_last_error()), which the Fortran
+ *    shim maps to err%equit (perrors_class.f03:96-118).
+ *  - Host arrays use the reference's column-major layouts:
+ *      real-space field  rf(dim, nx+2, 2*ny+1)    (ufield2d_class.f03:129)
+ *      k-space field     rf(dim, ny+1, nx+1)      (ufield2d_class.f03:198)
+ *      tiled particles   ppart(8, nppmx, ntiles), kpic(ntiles)
+ *                        (part2d_class.f03:170; tiles of 16 x 16 cells)
+ *      beam particles    part(7, np)              (part3d_class.f03)
+ *      3D field          rf(dim, nx+2, ny+1, nz+1) (ufield3d_class.f03:116)
+ *  - A field keeps the reference's state flag (0 = real space, 1 = Fourier
+ *    space, field2d_class.f03:24-26); operations check it like the reference
+ *    and fail with "data is in ks" / "data is in rs" otherwise.
+ *  - Calls on one context are stream-ordered on the context's CUDA stream.
+ *    One host thread per context.
+ */
+#ifndef QPGPU_H
+#define QPGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qp_ctx qp_ctx;
+typedef struct qp_field2d qp_field2d;
+typedef struct qp_species qp_species;
+typedef struct qp_beam qp_beam;
+typedef struct qp_sim qp_sim;
+
+/* ------------------------------------------------------------- context */
+
+/* Grid description: the simulation.{indx,indy,indz,box} keys of the input
+ * deck (simulation_class.f03:171-184).  4 <= indx, indy <= 11. */
+typedef struct {
+  int indx, indy, indz;
+  double box[3][2]; /* box.x(1:2), box.y(1:2), box.z(1:2) in c/wp */
+} qp_grid_desc;
+
+/* Creates a context on CUDA device `device` (replaces the per-rank set-up of
+ * simulation%new for one rank and one stage, simulation_class.f03:151-224). */
+int qp_ctx_create(const qp_grid_desc* grid, int device, qp_ctx** out);
+int qp_ctx_destroy(qp_ctx* ctx);
+/* Blocks until all work queued on the context has finished. */
+int qp_ctx_sync(qp_ctx* ctx);
+/* Required capacity after a call returned > 0. */
+long long qp_ctx_last_need(const qp_ctx* ctx);
+/* Message of the last failed call (static storage of the context). */
+const char* qp_ctx_last_error(const qp_ctx* ctx);
+/* dex = dx (transverse cell size) and dxi = dz (slice width) in c/wp. */
+int qp_ctx_spacing(const qp_ctx* ctx, float* dex, float* dxi);
+/* Device-time stopwatch on the context's stream (no reference counterpart;
+ * the reference logs wall-clock stamps, perrors_class.f03:120-134):
+ * start records an event, stop records a second one, waits for it and
+ * returns the elapsed milliseconds. */
+int qp_ctx_timer_start(qp_ctx* ctx);
+int qp_ctx_timer_stop(qp_ctx* ctx, double* ms);
+
+/* -------------------------------------------------------------- field2d */
+
+/* field2d%new (field2d_class.f03:82-138) with fftflag = .true.: dim = 1..3
+ * components, state = 0 (real space) or 1 (Fourier space). */
+int qp_field2d_create(qp_ctx* ctx, int dim, int state, qp_field2d** out);
+int qp_field2d_destroy(qp_field2d* f);
+int qp_field2d_state(const qp_field2d* f);
+int qp_field2d_dim(const qp_field2d* f);
+/* Copy real-space data rf(dim, nx+2, 2*ny+1) in / out; upload sets state 0. */
+int qp_field2d_upload_rs(qp_field2d* f, const float* rf);
+int qp_field2d_download_rs(qp_field2d* f, float* rf);
+/* Copy Fourier-space data rf(dim, ny+1, nx+1) in / out; upload sets state 1. */
+int qp_field2d_upload_ks(qp_field2d* f, const float* kf);
+int qp_field2d_download_ks(qp_field2d* f, float* kf);
+
+/* field2d%fftrk / %fftkr (field2d_class.f03:157-227): kind 1, 2, 3 select the
+ * sine/cosine parities of fft2d%fsst / %fcct / %fs3t (fft2d_class.f03:121-413).
+ * fftkr ends with the guard copy (ufield2d copyguard). */
+int qp_field2d_fftrk(qp_field2d* f, int kind);
+int qp_field2d_fftkr(qp_field2d* f, int kind);
+
+/* Fourier-space solves; `src` must be in state 1, `dst` is left in state 1. */
+int qp_field2d_pot(qp_field2d* src, qp_field2d* dst);    /* MPPOTPD2 via field2d%pot 295-316 */
+int qp_field2d_smooth(qp_field2d* src, qp_field2d* dst); /* MPPSMOOTHD2 via field2d%smooth 341-362 */
+int qp_field2d_elf(qp_field2d* src, qp_field2d* dst);    /* MPPOISD22 via field2d%elf 364-385 */
+int qp_field2d_bf(qp_field2d* src, qp_field2d* dst);     /* MPPBBPOISD23 via field2d%bf 387-408 */
+int qp_field2d_div(qp_field2d* src, qp_field2d* dst);    /* MPPDIVFD2 via field2d%div 229-249 */
+int qp_field2d_grad(qp_field2d* src, qp_field2d* dst);   /* MPPGRADFD2 via field2d%grad 251-271 */
+/* field2d%bfqp (field2d_class.f03:410-432 -> PBPOISD22N_QP): the transverse-B
+ * corrector; dcu is modified in place, bxy (2 components) is read and written. */
+int qp_field2d_bfqp(qp_field2d* cu, qp_field2d* dcu, qp_field2d* amu, qp_field2d* bxy, float c,
+                    float dex);
+
+/* Field algebra of field2d/ufield2d (ufield2d_class.f03:558-811), applied to
+ * the real- or Fourier-space data according to the operands' state.
+ * Component lists are 1-based like the Fortran (/1,2/) arrays. */
+int qp_field2d_as(qp_field2d* f, float value);                    /* asc: rs = value, state 0 */
+int qp_field2d_copy(qp_field2d* dst, qp_field2d* src);            /* asa */
+int qp_field2d_add(qp_field2d* dst, qp_field2d* a1, qp_field2d* a2);       /* sum1 */
+int qp_field2d_sub(qp_field2d* dst, qp_field2d* a1, qp_field2d* a2);       /* minus1 */
+int qp_field2d_mult(qp_field2d* dst, qp_field2d* a1, float value);         /* multiply1 */
+int qp_field2d_add_comp(qp_field2d* dst, qp_field2d* a1, qp_field2d* a2, const int* dim,
+                        const int* dim1, const int* dim2, int n);          /* sum2 */
+int qp_field2d_sub_comp(qp_field2d* dst, qp_field2d* a1, qp_field2d* a2, const int* dim,
+                        const int* dim1, const int* dim2, int n);          /* minus2 */
+int qp_field2d_mult_comp(qp_field2d* dst, qp_field2d* a1, const int* dim, const int* dim1,
+                         const float* value, int n);                       /* multiply2 */
+int qp_field2d_cg(qp_field2d* f); /* copyguard: row ny = row 0 (ufield2d_lib.f03:37-42) */
+int qp_field2d_ag(qp_field2d* f); /* acopyguard: row 0 += row ny (ufield2d_lib.f03:90-97) */
+
+/* ------------------------------------------------------------ species2d */
+
+/* Plasma species of profile 0 (uniform, fdist2d_000, fdist2d_class.f03:164-316)
+ * with the keys species(i).{ppc, q, m, density}; xtras is part2d's buffer
+ * headroom (0.2 in the reference, part2d_class.f03:62). */
+typedef struct {
+  int profile;
+  int ppc[2];
+  float q, m, density;
+  float xtras;
+} qp_species_desc;
+
+/* species2d%new (species2d_class.f03:74-118): loads and bins the particles
+ * (PPDBLKP2L, PPPMOVIN2L, PPPCHECK2L) and forms the ion background qn. */
+int qp_species_create(qp_ctx* ctx, const qp_species_desc* d, float s, qp_species** out);
+int qp_species_destroy(qp_species* sp);
+/* species2d%renew (species2d_class.f03:138-164): fresh plasma for the next 3D step. */
+int qp_species_renew(qp_species* sp, float s);
+/* species2d%qdp (166-185): q_species = deposit (PPGPPOST2L) + guard add;
+ * qe = q_species + qe; qe = qn + qe.  qe must be in state 0. */
+int qp_species_qdp(qp_species* sp, qp_field2d* qe);
+/* species2d%extpsi (256-272 -> WPGPSIPOST2L_QP). */
+int qp_species_extpsi(qp_species* sp, qp_field2d* psi, float dex);
+/* species2d%amjdp (187-218 -> PPGRDCJPPOST2L_QP): adds the species' current,
+ * acceleration and momentum-flux densities to cu, dcu, amu (state 0). */
+int qp_species_amjdp(qp_species* sp, qp_field2d* fxy, qp_field2d* bxyz, qp_field2d* psit,
+                     qp_field2d* cu, qp_field2d* amu, qp_field2d* dcu, float dex);
+/* species2d%push (220-237) = part2d%partpush (PPGRBPPUSHF23L_QP) + pmove. */
+int qp_species_push(qp_species* sp, qp_field2d* fxy, qp_field2d* bxyz, qp_field2d* psit,
+                    float dex);
+/* The two halves of push: part2d%partpush (part2d_class.f03:315-358, in place,
+ * no re-binning) and part2d%pmove (360-594, re-binning into tiles). */
+int qp_species_partpush(qp_species* sp, qp_field2d* fxy, qp_field2d* bxyz, qp_field2d* psit,
+                        float dex);
+int qp_species_pmove(qp_species* sp);
+/* species2d%cbq (399-418): q_species(1) += cu_species(3); smooth; store as
+ * slice `pos` (1-based) of the species' 3D charge q3. */
+int qp_species_cbq(qp_species* sp, int pos);
+/* Particle data in the reference's tiled layout: ppart(8, nppmx_ld, ntiles),
+ * kpic(ntiles).  nppmx_ld must be >= qp_species_nppmx(). */
+int qp_species_ntiles(const qp_species* sp);
+int qp_species_nppmx(const qp_species* sp);
+long long qp_species_np(qp_species* sp);
+int qp_species_download(qp_species* sp, float* ppart, int* kpic, int nppmx_ld);
+int qp_species_upload(qp_species* sp, const float* ppart, const int* kpic, int nppmx_ld);
+/* The ion background qn (real space, (1, nx+2, 2*ny+1)) and the species'
+ * own charge density q after the last qdp/cbq. */
+int qp_species_download_qn(qp_species* sp, float* rf);
+int qp_species_download_q(qp_species* sp, float* rf);
+/* Slice `pos` (1-based) of the species' 3D smoothed charge q3 as (nx+2, ny+1). */
+int qp_species_download_q3(qp_species* sp, int pos, float* rf);
+
+/* --------------------------------------------------------------- beam3d */
+
+/* Tri-Gaussian beam, profile 0 (fdist3d_000, fdist3d_class.f03:222-421) with
+ * the keys beam(i).{np, q, m, gamma, peak_density, quiet_start, center, sigma,
+ * sigma_v, npmax}; loaded with PRVDIST32_RANDOM and ranorm's fixed seeds
+ * (part3d_lib77.f:411-552, 1324-1383).  Beams created on one context draw
+ * from one ranorm sequence, in creation order, like the reference. */
+typedef struct {
+  int profile;
+  int np[3];
+  float q, m, gamma, peak_density;
+  int quiet_start;
+  float center[3], sigma[3], sigma_v[3];
+  long long npmax;
+} qp_beam_desc;
+
+int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out);
+int qp_beam_destroy(qp_beam* b);
+long long qp_beam_np(const qp_beam* b);
+/* beam3d%qdp (beam3d_class.f03:111-134 -> PGPOST32L): 3D charge deposit. */
+int qp_beam_qdp(qp_beam* b);
+/* beam3d%qdp(q, slice) (qdpcopy_beam3d 136-153): q(rs) += slice `slice`
+ * (1-based) of the beam's 3D charge; q must be in state 0. */
+int qp_beam_qdpcopy(qp_beam* b, qp_field2d* q, int slice);
+int qp_beam_download(qp_beam* b, float* part /* (7, np) */);
+/* Replace the beam's particles with part(7, np) from host memory (np must
+ * equal qp_beam_np); the restart read of beam particles, part3d%rrst
+ * (part3d_class.f03:315-331), without the HDF5 file. */
+int qp_beam_upload(qp_beam* b, const float* part, long long np);
+int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
+
+/* ----------------------------------------------------- fused 3D step */
+
+/* The whole 3D step of go_simulation (simulation_class.f03:611-764) for the
+ * species and beams given, with all state on the GPU: beam deposit, the
+ * per-slice loop (643-736) captured as CUDA graphs, and the species renew.
+ * iter = fixed number of B predictor-corrector passes (simulation.iter);
+ * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3. */
+typedef struct {
+  int iter;
+  int store3d;
+  int use_graphs;
+  int reserved[5];
+} qp_sim_desc;
+
+typedef struct {
+  int slices;          /* slices advanced */
+  int iterations;      /* predictor-corrector passes run */
+  int regrowths;       /* particle-buffer growths (overflow recoveries) */
+  int kernels;         /* kernel launches of the step */
+  double gpu_ms;       /* device time of the step */
+} qp_step_stats;
+
+int qp_sim_create(qp_ctx* ctx, const qp_sim_desc* d, qp_species* const* species, int nspecies,
+                  qp_beam* const* beams, int nbeams, qp_sim** out);
+int qp_sim_destroy(qp_sim* sim);
+/* One 3D step; `stats` may be NULL.  The species are renewed at the end. */
+int qp_sim_step3d(qp_sim* sim, qp_step_stats* stats);
+/* Fields of the last slice (real space or Fourier space, reference layout):
+ * name = "psi", "fxy", "bxyz", "psit", "cu", "dcu", "amu" (rs) or
+ * "epw", "cu_k", "epwb" (ks). */
+int qp_sim_download_field(qp_sim* sim, const char* name, float* out);
+/* 3D fields (3, nx+2, ny+1, nz+1): "bexyz" or "bbxyz"; species 3D charge
+ * (nx+2, ny+1, nz+1): "q3". */
+int qp_sim_download_3d(qp_sim* sim, const char* name, float* out);
+/* Per-kernel device times of the first `nslices` slices of a 3D step, run
+ * without graphs with an event pair around every launch (the timing side of
+ * the reference's per-step ELOG stamps, simulation_class.f03:614-645).
+ * Kernel names are written newline-separated into `names`; ms[i], count[i] and
+ * bytes[i] are the total milliseconds, launches and algorithmic bytes
+ * (minimal FP32 traffic of the work done) of name i.  Returns the number of
+ * names (<= max), or < 0 on error.  The species are renewed afterwards. */
+int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double* ms, int* count,
+                   double* bytes, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,79 @@
+// qp_common.cuh -- shared definitions of the B200 quasi-static slice engine.
+//
+// Device data layout (all FP32, one plane per field component):
+//   real-space plane  R[y][x], y = 0..ny (row ny is the guard row), x = 0..nx+1,
+//                     row pitch rp = nx + 4 floats (16-byte aligned rows)
+//   k-space plane     K[kx][ky], kx = 0..nx, ky = 0..ny, pitch kp = ny + 4;
+//                     the same array holds the half-transformed data between
+//                     the x pass and the y pass ([kx][y])
+//   particles         structure of arrays: 8 planes (x, y, px, py, pz, p6, p7, q)
+//                     of ntiles * cap floats; tile t owns [t*cap, t*cap+count[t])
+// Grid nodes, tile size and the particle slots follow QuickPIC's part2d/ufield2d
+// (16 x 16 cell tiles, positions in cell units, node j at x = j).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+
+#define QP_MAX_IND 11  // largest supported log2 of a transverse grid size
+
+namespace qp {
+
+struct GridDims {
+  int indx, indy, nx, ny;
+  int rp;        // real-space row pitch (floats)
+  int kp;        // k-space column pitch (floats)
+  long long rplane;  // floats per real-space plane: (ny + 1) * rp
+  long long kplane;  // floats per k-space plane: (nx + 1) * kp
+};
+
+inline GridDims make_dims(int indx, int indy) {
+  GridDims d;
+  d.indx = indx;
+  d.indy = indy;
+  d.nx = 1 << indx;
+  d.ny = 1 << indy;
+  d.rp = d.nx + 4;
+  d.kp = d.ny + 4;
+  d.rplane = (long long)(d.ny + 1) * d.rp;
+  d.kplane = (long long)(d.nx + 1) * d.kp;
+  return d;
+}
+
+// Twiddle tables for one line length n (host-computed in double, stored FP32).
+struct LineTables {
+  const float* sn;   // sin(pi j / n), j = 0..n
+  const float* cs;   // cos(pi j / n), j = 0..n
+  const float2* tw;  // exp(-2 pi i m / (n/2)), m = 0..n/2-1  (complex FFT of n/2)
+  const float2* uw;  // exp(-2 pi i k / n),     k = 0..n/2    (real-FFT unscramble)
+};
+
+// Sticky device status shared by every kernel of a context.
+struct DevStatus {
+  int error;          // 0 = ok; >0 = capacity overflow (see need); <0 = fatal
+  int fail_slice;     // slice index at which the first error was raised
+  int need_cap;       // particles a tile must hold
+  int need_inbox;     // movers a tile must accept
+  int cursor;         // slice cursor of the fused 3D step
+  int iter_done;      // iterations run in the current slice
+  int pad[2];
+  float resid_num;    // convergence residual accumulators
+  float resid_den;
+};
+
+enum { QP_OK = 0, QP_OVERFLOW = 1 };
+
+}  // namespace qp
+
+#define QP_CUDA_CHECK(call)                                                         \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      qp_set_error(__FILE__, __LINE__, cudaGetErrorString(e_));                     \
+      return -2;                                                                    \
+    }                                                                               \
+  } while (0)
+
+void qp_set_error(const char* file, int line, const char* msg);

@@ -1,0 +1,463 @@
+"""qpgpu -- Python host side of the B200 QuickPIC slice engine.
+
+The engine is the shared library ``libqpgpu.so`` next to this file (C ABI in
+``include/qpgpu.h``).  This module binds it with ctypes and mirrors the
+reference's Fortran class interface for the per-slice path, with the same
+method names and argument meaning:
+
+* :class:`Field2d`   -- ``field2d`` (fftrk/fftkr/pot/grad/div/elf/bf/bfqp/smooth,
+  as/add/sub/mult, cg/ag)  (QuickPIC source/field2d_class.f03)
+* :class:`Species2d` -- ``species2d`` (qdp/extpsi/amjdp/push/renew/cbq)
+  (source/species2d_class.f03)
+* :class:`Beam3d`    -- ``beam3d`` (qdp, qdp(q, slice))  (source/beam3d_class.f03)
+* :class:`Simulation` -- the fused 3D step of ``simulation%go``
+  (source/simulation_class.f03:593-769) with all state on the GPU.
+
+Errors: a negative return code of the library raises :class:`QPError` (the
+reference's ``err%equit``); capacity overflows are recovered inside the
+library by growing the buffers, as ``part2d%pmove`` does.
+
+There is no CPU fallback: importing this module without the built library, or
+calling it without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqpgpu.so")
+
+__all__ = ["QPError", "Context", "Field2d", "Species2d", "Beam3d", "Simulation", "lib",
+           "build", "exported_symbols", "LIB_PATH"]
+
+
+class QPError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def build() -> str:
+    """Compile libqpgpu.so for sm_100a with the package Makefile."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", os.path.dirname(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QPError(f"{LIB_PATH} is missing: build it with `make -C "
+                          f"{os.path.dirname(HERE)}` (there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        L.qp_ctx_last_error.restype = C.c_char_p
+        L.qp_ctx_last_need.restype = C.c_longlong
+        L.qp_species_np.restype = C.c_longlong
+        L.qp_beam_np.restype = C.c_longlong
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names of the qp_* functions declared in include/qpgpu.h."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "qpgpu.h")
+    txt = open(hdr).read()
+    return sorted(set(re.findall(r"\b(qp_[a-z0-9_]+)\s*\(", txt)))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class _GridDesc(C.Structure):
+    _fields_ = [("indx", C.c_int), ("indy", C.c_int), ("indz", C.c_int),
+                ("box", (C.c_double * 2) * 3)]
+
+
+class _SpeciesDesc(C.Structure):
+    _fields_ = [("profile", C.c_int), ("ppc", C.c_int * 2), ("q", C.c_float), ("m", C.c_float),
+                ("density", C.c_float), ("xtras", C.c_float)]
+
+
+class _BeamDesc(C.Structure):
+    _fields_ = [("profile", C.c_int), ("np", C.c_int * 3), ("q", C.c_float), ("m", C.c_float),
+                ("gamma", C.c_float), ("peak_density", C.c_float), ("quiet_start", C.c_int),
+                ("center", C.c_float * 3), ("sigma", C.c_float * 3),
+                ("sigma_v", C.c_float * 3), ("npmax", C.c_longlong)]
+
+
+class _SimDesc(C.Structure):
+    _fields_ = [("iter", C.c_int), ("store3d", C.c_int), ("use_graphs", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("slices", C.c_int), ("iterations", C.c_int), ("regrowths", C.c_int),
+                ("kernels", C.c_int), ("gpu_ms", C.c_double)]
+
+
+class Context:
+    """One GPU context for a grid of 2**indx x 2**indy x 2**indz cells."""
+
+    def __init__(self, indx, indy, indz, box, device=0):
+        g = _GridDesc()
+        g.indx, g.indy, g.indz = indx, indy, indz
+        for a in range(3):
+            g.box[a][0], g.box[a][1] = box[a]
+        h = C.c_void_p()
+        self._L = lib()
+        self._check(self._L.qp_ctx_create(C.byref(g), device, C.byref(h)), ctx=None)
+        self.h = h
+        self.indx, self.indy, self.indz = indx, indy, indz
+        self.nx, self.ny, self.nz = 1 << indx, 1 << indy, 1 << indz
+        dex, dxi = C.c_float(), C.c_float()
+        self._L.qp_ctx_spacing(self.h, C.byref(dex), C.byref(dxi))
+        self.dex, self.dxi = dex.value, dxi.value
+
+    def _check(self, rc, ctx="self"):
+        if rc < 0:
+            c = self.h if ctx == "self" else None
+            msg = self._L.qp_ctx_last_error(c)
+            raise QPError(msg.decode() if msg else f"qpgpu error {rc}")
+        return rc
+
+    def sync(self):
+        self._check(self._L.qp_ctx_sync(self.h))
+
+    def timer_start(self):
+        """Record a start event on the engine's stream."""
+        self._check(self._L.qp_ctx_timer_start(self.h))
+
+    def timer_stop(self):
+        """Record a stop event, wait for it, return device milliseconds since start."""
+        ms = C.c_double()
+        self._check(self._L.qp_ctx_timer_stop(self.h, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.qp_ctx_destroy(self.h)
+            self.h = None
+
+    # reference layouts
+    def rs_shape(self, dim):
+        return (dim, self.nx + 2, 2 * self.ny + 1)
+
+    def ks_shape(self, dim):
+        return (dim, self.ny + 1, self.nx + 1)
+
+
+class Field2d:
+    """field2d: a real-space / Fourier-space pair with the reference's state flag."""
+
+    def __init__(self, ctx: Context, dim, state=0):
+        self.ctx, self.dim = ctx, dim
+        h = C.c_void_p()
+        ctx._check(ctx._L.qp_field2d_create(ctx.h, dim, state, C.byref(h)))
+        self.h = h
+
+    @property
+    def state(self):
+        return self.ctx._L.qp_field2d_state(self.h)
+
+    def _c(self, rc):
+        return self.ctx._check(rc)
+
+    # data movement
+    def set_rs(self, a):
+        a = np.asfortranarray(a, dtype=np.float32).reshape(self.ctx.rs_shape(self.dim), order="F")
+        self._c(self.ctx._L.qp_field2d_upload_rs(self.h, _ptr(a)))
+
+    def get_rs(self):
+        out = np.zeros(self.ctx.rs_shape(self.dim), dtype=np.float32, order="F")
+        self._c(self.ctx._L.qp_field2d_download_rs(self.h, _ptr(out)))
+        return out
+
+    def set_ks(self, a):
+        a = np.asfortranarray(a, dtype=np.float32).reshape(self.ctx.ks_shape(self.dim), order="F")
+        self._c(self.ctx._L.qp_field2d_upload_ks(self.h, _ptr(a)))
+
+    def get_ks(self):
+        out = np.zeros(self.ctx.ks_shape(self.dim), dtype=np.float32, order="F")
+        self._c(self.ctx._L.qp_field2d_download_ks(self.h, _ptr(out)))
+        return out
+
+    # field2d methods
+    def fftrk(self, kind):
+        self._c(self.ctx._L.qp_field2d_fftrk(self.h, kind))
+
+    def fftkr(self, kind):
+        self._c(self.ctx._L.qp_field2d_fftkr(self.h, kind))
+
+    def pot(self, that):
+        self._c(self.ctx._L.qp_field2d_pot(self.h, that.h))
+
+    def smooth(self, that):
+        self._c(self.ctx._L.qp_field2d_smooth(self.h, that.h))
+
+    def elf(self, that):
+        self._c(self.ctx._L.qp_field2d_elf(self.h, that.h))
+
+    def bf(self, that):
+        self._c(self.ctx._L.qp_field2d_bf(self.h, that.h))
+
+    def div(self, that):
+        self._c(self.ctx._L.qp_field2d_div(self.h, that.h))
+
+    def grad(self, that):
+        self._c(self.ctx._L.qp_field2d_grad(self.h, that.h))
+
+    def bfqp(self, dcu, amu, bxy, c, dex):
+        self._c(self.ctx._L.qp_field2d_bfqp(self.h, dcu.h, amu.h, bxy.h, C.c_float(c),
+                                            C.c_float(dex)))
+
+    def as_(self, value):
+        self._c(self.ctx._L.qp_field2d_as(self.h, C.c_float(value)))
+
+    def copy_from(self, that):
+        self._c(self.ctx._L.qp_field2d_copy(self.h, that.h))
+
+    def add(self, a1, a2, dim=None, dim1=None, dim2=None):
+        if dim is None:
+            self._c(self.ctx._L.qp_field2d_add(self.h, a1.h, a2.h))
+        else:
+            d, d1, d2 = (np.asarray(v, dtype=np.int32) for v in (dim, dim1, dim2))
+            self._c(self.ctx._L.qp_field2d_add_comp(self.h, a1.h, a2.h, _ptr(d), _ptr(d1),
+                                                    _ptr(d2), len(d)))
+
+    def sub(self, a1, a2, dim=None, dim1=None, dim2=None):
+        if dim is None:
+            self._c(self.ctx._L.qp_field2d_sub(self.h, a1.h, a2.h))
+        else:
+            d, d1, d2 = (np.asarray(v, dtype=np.int32) for v in (dim, dim1, dim2))
+            self._c(self.ctx._L.qp_field2d_sub_comp(self.h, a1.h, a2.h, _ptr(d), _ptr(d1),
+                                                    _ptr(d2), len(d)))
+
+    def mult(self, a1, value, dim=None, dim1=None):
+        if dim is None:
+            self._c(self.ctx._L.qp_field2d_mult(self.h, a1.h, C.c_float(value)))
+        else:
+            d, d1 = (np.asarray(v, dtype=np.int32) for v in (dim, dim1))
+            v = np.asarray(value, dtype=np.float32)
+            self._c(self.ctx._L.qp_field2d_mult_comp(self.h, a1.h, _ptr(d), _ptr(d1), _ptr(v),
+                                                     len(d)))
+
+    def cg(self):
+        self._c(self.ctx._L.qp_field2d_cg(self.h))
+
+    def ag(self):
+        self._c(self.ctx._L.qp_field2d_ag(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.qp_field2d_destroy(self.h)
+            self.h = None
+
+
+class Species2d:
+    """species2d with a uniform (profile 0) plasma."""
+
+    def __init__(self, ctx: Context, ppc=(2, 2), q=-1.0, m=1.0, density=1.0, xtras=0.2, s=0.0):
+        d = _SpeciesDesc()
+        d.profile = 0
+        d.ppc[0], d.ppc[1] = ppc
+        d.q, d.m, d.density, d.xtras = q, m, density, xtras
+        h = C.c_void_p()
+        ctx._check(ctx._L.qp_species_create(ctx.h, C.byref(d), C.c_float(s), C.byref(h)))
+        self.ctx, self.h = ctx, h
+        self.qbm = q / m
+        self.dt = ctx.dxi
+
+    def _c(self, rc):
+        return self.ctx._check(rc)
+
+    @property
+    def ntiles(self):
+        return self.ctx._L.qp_species_ntiles(self.h)
+
+    @property
+    def nppmx(self):
+        return self.ctx._L.qp_species_nppmx(self.h)
+
+    def np(self):
+        return int(self.ctx._L.qp_species_np(self.h))
+
+    def qdp(self, qe):
+        self._c(self.ctx._L.qp_species_qdp(self.h, qe.h))
+
+    def extpsi(self, psi, dex):
+        self._c(self.ctx._L.qp_species_extpsi(self.h, psi.h, C.c_float(dex)))
+
+    def amjdp(self, fxy, bxyz, psit, cu, amu, dcu, dex):
+        self._c(self.ctx._L.qp_species_amjdp(self.h, fxy.h, bxyz.h, psit.h, cu.h, amu.h, dcu.h,
+                                             C.c_float(dex)))
+
+    def push(self, fxy, bxyz, psit, dex):
+        self._c(self.ctx._L.qp_species_push(self.h, fxy.h, bxyz.h, psit.h, C.c_float(dex)))
+
+    def partpush(self, fxy, bxyz, psit, dex):
+        self._c(self.ctx._L.qp_species_partpush(self.h, fxy.h, bxyz.h, psit.h, C.c_float(dex)))
+
+    def pmove(self):
+        self._c(self.ctx._L.qp_species_pmove(self.h))
+
+    def renew(self, s=0.0):
+        self._c(self.ctx._L.qp_species_renew(self.h, C.c_float(s)))
+
+    def cbq(self, pos):
+        self._c(self.ctx._L.qp_species_cbq(self.h, pos))
+
+    def get_particles(self, nppmx=None):
+        """(ppart(8, nppmx, ntiles), kpic(ntiles)) in the reference layout."""
+        nppmx = nppmx or self.nppmx
+        pp = np.zeros((8, nppmx, self.ntiles), dtype=np.float32, order="F")
+        kp = np.zeros(self.ntiles, dtype=np.int32)
+        self._c(self.ctx._L.qp_species_download(self.h, _ptr(pp), _ptr(kp), nppmx))
+        return pp, kp
+
+    def set_particles(self, ppart, kpic):
+        pp = np.asfortranarray(ppart, dtype=np.float32)
+        kp = np.ascontiguousarray(kpic, dtype=np.int32)
+        self._c(self.ctx._L.qp_species_upload(self.h, _ptr(pp), _ptr(kp), pp.shape[1]))
+
+    def get_qn(self):
+        out = np.zeros(self.ctx.rs_shape(1), dtype=np.float32, order="F")
+        self._c(self.ctx._L.qp_species_download_qn(self.h, _ptr(out)))
+        return out
+
+    def get_q(self):
+        out = np.zeros(self.ctx.rs_shape(1), dtype=np.float32, order="F")
+        self._c(self.ctx._L.qp_species_download_q(self.h, _ptr(out)))
+        return out
+
+    def get_q3(self, pos):
+        out = np.zeros((self.ctx.nx + 2, self.ctx.ny + 1), dtype=np.float32, order="F")
+        self._c(self.ctx._L.qp_species_download_q3(self.h, pos, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.qp_species_destroy(self.h)
+            self.h = None
+
+
+class Beam3d:
+    """beam3d with a tri-Gaussian (profile 0) distribution."""
+
+    def __init__(self, ctx: Context, np3, q=-1.0, m=1.0, gamma=20000.0, peak_density=1.0,
+                 quiet_start=True, center=(0, 0, 0), sigma=(1, 1, 1), sigma_v=(0, 0, 0),
+                 npmax=0):
+        d = _BeamDesc()
+        d.profile = 0
+        for a in range(3):
+            d.np[a] = int(np3[a])
+            d.center[a], d.sigma[a], d.sigma_v[a] = center[a], sigma[a], sigma_v[a]
+        d.q, d.m, d.gamma, d.peak_density = q, m, gamma, peak_density
+        d.quiet_start = 1 if quiet_start else 0
+        d.npmax = int(npmax)
+        h = C.c_void_p()
+        ctx._check(ctx._L.qp_beam_create(ctx.h, C.byref(d), C.byref(h)))
+        self.ctx, self.h = ctx, h
+
+    def np(self):
+        return int(self.ctx._L.qp_beam_np(self.h))
+
+    def qdp(self, q=None, slice=None):
+        if q is None:
+            self.ctx._check(self.ctx._L.qp_beam_qdp(self.h))
+        else:
+            self.ctx._check(self.ctx._L.qp_beam_qdpcopy(self.h, q.h, slice))
+
+    def get_particles(self):
+        out = np.zeros((7, self.np()), dtype=np.float32, order="F")
+        self.ctx._check(self.ctx._L.qp_beam_download(self.h, _ptr(out)))
+        return out
+
+    def set_particles(self, part):
+        """Upload part(7, np) (Fortran order, float32; pinned memory makes it async)."""
+        assert part.dtype == np.float32 and part.flags["F_CONTIGUOUS"] and part.shape[0] == 7
+        self.ctx._check(self.ctx._L.qp_beam_upload(self.h, _ptr(part),
+                                                   C.c_longlong(part.shape[1])))
+
+    def get_q3d(self):
+        c = self.ctx
+        out = np.zeros((c.nx + 2, c.ny + 1, c.nz + 1), dtype=np.float32, order="F")
+        c._check(c._L.qp_beam_download_q3d(self.h, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.qp_beam_destroy(self.h)
+            self.h = None
+
+
+class Simulation:
+    """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
+
+    def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=True):
+        d = _SimDesc()
+        d.iter = iter
+        d.store3d = 1 if store3d else 0
+        d.use_graphs = 1 if use_graphs else 0
+        sp = (C.c_void_p * len(species))(*[s.h for s in species])
+        bm = (C.c_void_p * max(len(beams), 1))(*[b.h for b in beams])
+        h = C.c_void_p()
+        ctx._check(ctx._L.qp_sim_create(ctx.h, C.byref(d), sp, len(species), bm, len(beams),
+                                        C.byref(h)))
+        self.ctx, self.h = ctx, h
+        self.species, self.beams = species, beams
+
+    def step3d(self) -> StepStats:
+        st = StepStats()
+        self.ctx._check(self.ctx._L.qp_sim_step3d(self.h, C.byref(st)))
+        return st
+
+    def get_field(self, name):
+        c = self.ctx
+        dims = dict(psi=1, fxy=2, bxyz=3, psit=1, cu=3, dcu=2, amu=3, epw=2, cu_k=3, epwb=2)
+        dim = dims[name]
+        shape = c.ks_shape(dim) if name in ("epw", "cu_k", "epwb") else c.rs_shape(dim)
+        out = np.zeros(shape, dtype=np.float32, order="F")
+        c._check(c._L.qp_sim_download_field(self.h, name.encode(), _ptr(out)))
+        return out
+
+    def get_3d(self, name):
+        c = self.ctx
+        if name == "q3":
+            shape = (c.nx + 2, c.ny + 1, c.nz + 1)
+        else:
+            shape = (3, c.nx + 2, c.ny + 1, c.nz + 1)
+        out = np.zeros(shape, dtype=np.float32, order="F")
+        c._check(c._L.qp_sim_download_3d(self.h, name.encode(), _ptr(out)))
+        return out
+
+    def lineout(self, comp=3, out=None):
+        """On-axis bexyz(comp) for every slice (nz+1 values)."""
+        if out is None:
+            out = np.zeros(self.ctx.nz + 1, dtype=np.float32)
+        self.ctx._check(self.ctx._L.qp_sim_download_lineout(self.h, comp, _ptr(out)))
+        return out
+
+    def profile(self, nslices):
+        """{kernel name: (total ms, launches, algorithmic bytes)} over nslices slices."""
+        buf = C.create_string_buffer(4096)
+        ms = (C.c_double * 64)()
+        cnt = (C.c_int * 64)()
+        byt = (C.c_double * 64)()
+        n = self.ctx._check(self.ctx._L.qp_sim_profile(self.h, nslices, buf, 4096, ms, cnt, byt,
+                                                       64))
+        names = buf.value.decode().split("\n")[:n]
+        return {names[i]: (ms[i], cnt[i], byt[i]) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.qp_sim_destroy(self.h)
+            self.h = None

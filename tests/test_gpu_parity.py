@@ -1,0 +1,384 @@
+"""Parity of the B200 engine with the CPU oracle, kernel by kernel and for whole slices.
+
+Every test feeds the engine (through the C ABI) and the oracle the same inputs
+in the reference's layouts.  Tolerances (relative L2 unless stated):
+  * transforms and Fourier-space solves: 2e-5 against the FP32 oracle (whose own
+    NR transforms carry ~5e-6 of FP32 roundoff) and 1e-5 against the FP64 oracle;
+  * particle kernels: per particle, 2e-6 relative / 1e-6 absolute (FMA contraction
+    on the GPU is the only difference in the arithmetic);
+  * deposits: 1e-6 (shared-memory and edge atomics change the summation order);
+  * re-binning: bit-exact per tile (it only moves data);
+  * whole slices: 1e-4 on fields after several slices (the roundoff above feeds
+    back through the particle orbits), and atomic-order nondeterminism is measured.
+"""
+import numpy as np
+import pytest
+from conftest import make_config, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_FFT32, TOL_FFT64 = 2e-5, 1e-5
+
+
+@pytest.fixture(scope="module")
+def qp():
+    import qpgpu
+
+    return qpgpu
+
+
+@pytest.fixture(scope="module")
+def ctx(qp):
+    c = qp.Context(6, 6, 5, [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]])
+    yield c
+    c.close()
+
+
+def _rand_rs(O, dim, ix, iy, seed, dtype=np.float32):
+    nx, ny = 1 << ix, 1 << iy
+    rng = np.random.default_rng(seed)
+    rs = O.rs_zeros(dim, ix, iy, dtype)
+    rs[:, : nx + 1, : ny + 1] = rng.standard_normal((dim, nx + 1, ny + 1))
+    return rs
+
+
+KINDS = [(1, 1), (2, 1), (1, 2), (2, 2), (1, 3), (2, 3), (3, 3)]
+
+
+@pytest.mark.parametrize("kind,dim", KINDS)
+def test_fftrk_fftkr(qp, ctx, oracle_mod, kind, dim):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    rs = _rand_rs(O, dim, ix, iy, 100 * kind + dim)
+    f = qp.Field2d(ctx, dim, 0)
+    f.set_rs(rs)
+    f.fftrk(kind)
+    gk = f.get_ks()
+    ks32 = O.ks_zeros(dim, ix, iy, np.float32)
+    r32 = rs.copy()
+    O.fftrk(r32, ks32, kind, ix, iy)
+    ks64 = O.ks_zeros(dim, ix, iy, np.float64)
+    r64 = rs.astype(np.float64)
+    O.fftrk(r64, ks64, kind, ix, iy)
+    assert rel_l2(gk, ks64) < TOL_FFT64
+    assert rel_l2(gk, ks32) < TOL_FFT32
+    # inverse from the same k-space data
+    f.set_ks(ks64.astype(np.float32))
+    f.fftkr(kind)
+    gr = f.get_rs()
+    k64 = ks64.copy()
+    O.fftkr(r64, k64, kind, ix, iy)
+    ny = 1 << iy
+    assert rel_l2(gr[:, :, : ny + 1], r64[:, :, : ny + 1]) < TOL_FFT64
+    assert np.array_equal(gr[:, :, ny], gr[:, :, 0])  # copyguard
+    f.close()
+
+
+def test_fft_rectangular_grid(qp, oracle_mod):
+    O = oracle_mod
+    c = qp.Context(7, 5, 4, [[-6.0, 6.0], [-3.0, 3.0], [0.0, 10.0]])
+    for kind, dim in ((1, 3), (2, 3)):
+        rs = _rand_rs(O, dim, 7, 5, 7 + kind)
+        f = qp.Field2d(c, dim, 0)
+        f.set_rs(rs)
+        f.fftrk(kind)
+        k64 = O.ks_zeros(dim, 7, 5, np.float64)
+        O.fftrk(rs.astype(np.float64), k64, kind, 7, 5)
+        assert rel_l2(f.get_ks(), k64) < TOL_FFT64
+        f.close()
+    c.close()
+
+
+def _rand_ks(O, dim, ix, iy, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(O.ks_zeros(dim, ix, iy).shape).astype(np.float32)
+
+
+def test_kspace_solves(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    t = O.ffc(ix, iy, np.float32)
+    q = _rand_ks(O, 1, ix, iy, 1)
+    cu = _rand_ks(O, 3, ix, iy, 2)
+    fq = qp.Field2d(ctx, 1, 1)
+    fq.set_ks(q)
+    fcu = qp.Field2d(ctx, 3, 1)
+    fcu.set_ks(cu)
+    out1, out2, out3 = qp.Field2d(ctx, 1, 1), qp.Field2d(ctx, 2, 1), qp.Field2d(ctx, 3, 1)
+    cases = [
+        ("pot", fq, out1, lambda o: O.pot(np.asfortranarray(q), o, t, ix, iy), 1),
+        ("smooth", fq, out1, lambda o: O.smooth(np.asfortranarray(q), o, t, ix, iy), 1),
+        ("elf", fq, out2, lambda o: O.elf(np.asfortranarray(q), o, t, ix, iy), 2),
+        ("grad", fq, out2, lambda o: O.grad(np.asfortranarray(q), o, ix, iy), 2),
+        ("bf", fcu, out3, lambda o: O.bf(np.asfortranarray(cu), o, t, ix, iy), 3),
+        ("div", fcu, out1, lambda o: O.div(np.asfortranarray(cu), o, ix, iy), 1),
+    ]
+    for name, src, dst, ref, dim in cases:
+        getattr(src, name)(dst)
+        exp = O.ks_zeros(dim, ix, iy, np.float32)
+        ref(exp)
+        got = dst.get_ks()
+        assert np.allclose(got, exp, rtol=2e-6, atol=1e-7), name
+    # bfqp: the transverse-B corrector (dcu modified in place)
+    dcu = _rand_ks(O, 2, ix, iy, 3)
+    amu = _rand_ks(O, 3, ix, iy, 4)
+    bxy = _rand_ks(O, 2, ix, iy, 5)
+    fd, fa, fb = qp.Field2d(ctx, 2, 1), qp.Field2d(ctx, 3, 1), qp.Field2d(ctx, 2, 1)
+    fd.set_ks(dcu)
+    fa.set_ks(amu)
+    fb.set_ks(bxy)
+    dex = ctx.dex
+    fcu.bfqp(fd, fa, fb, dex * dex, dex)
+    d_ref, b_ref = np.asfortranarray(dcu.copy()), np.asfortranarray(bxy.copy())
+    O.bfqp(np.asfortranarray(cu), d_ref, np.asfortranarray(amu), b_ref, t, dex * dex, dex, ix, iy)
+    assert np.allclose(fd.get_ks(), d_ref, rtol=2e-6, atol=1e-6)
+    assert np.allclose(fb.get_ks(), b_ref, rtol=2e-6, atol=1e-6)
+
+
+def _particles(O, ix, iy, seed, jitter=0.2, pscale=0.05):
+    part = O.dist2d_000(ix, iy, 2, 2, dtype=np.float32)
+    rng = np.random.default_rng(seed)
+    n = part.shape[1]
+    part[0] += rng.uniform(-jitter, jitter, n).astype(np.float32)
+    part[1] += rng.uniform(-jitter, jitter, n).astype(np.float32)
+    part[2:5] = rng.normal(0, pscale, (3, n)).astype(np.float32)
+    part[5] = 1.0 + rng.uniform(0, 0.1, n).astype(np.float32)
+    part[6] = 1.0 + rng.uniform(-0.05, 0.05, n).astype(np.float32)
+    return part
+
+
+def _fields(O, ctx, seed, amp=0.3):
+    ix, iy = ctx.indx, ctx.indy
+    fxy = _rand_rs(O, 2, ix, iy, seed) * amp
+    bxy = _rand_rs(O, 3, ix, iy, seed + 1) * amp
+    psit = _rand_rs(O, 1, ix, iy, seed + 2) * amp
+    ny = 1 << iy
+    for a in (fxy, bxy, psit):
+        a[:, :, ny] = a[:, :, 0]  # guard row as after fftkr
+    return fxy, bxy, psit
+
+
+def _upload_fields(qp, ctx, fxy, bxy, psit):
+    F = qp.Field2d(ctx, 2, 0)
+    F.set_rs(fxy)
+    B = qp.Field2d(ctx, 3, 0)
+    B.set_rs(bxy)
+    P = qp.Field2d(ctx, 1, 0)
+    P.set_rs(psit)
+    return F, B, P
+
+
+def _species_with(qp, ctx, pp, kp):
+    sp = qp.Species2d(ctx, ppc=(2, 2))
+    sp.set_particles(pp, kp)
+    return sp
+
+
+def _flat(pp, kp):
+    return np.concatenate([pp[:, : kp[t], t] for t in range(len(kp))], axis=1)
+
+
+def test_charge_deposit(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 11), ix, iy)
+    sp = _species_with(qp, ctx, pp, kp)
+    qe = qp.Field2d(ctx, 1, 0)
+    qe.as_(0.0)
+    sp.qdp(qe)
+    # oracle: q = deposit + guard add; qe = q + qe; qe = qn + qe
+    q = O.rs_zeros(1, ix, iy)
+    O.qdeposit(pp, kp, q, ix, iy)
+    O.acguard(q, ix, iy)
+    exp = q + sp.get_qn()
+    got = qe.get_rs()
+    assert rel_l2(got, exp) < 1e-6
+    assert np.isclose(got.sum(), (pp[7] * (np.arange(pp.shape[1])[:, None] < kp[None, :])).sum()
+                      + sp.get_qn().sum(), rtol=1e-5)
+
+
+def test_extpsi(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 12), ix, iy)
+    _, _, psi = _fields(O, ctx, 30)
+    sp = _species_with(qp, ctx, pp, kp)
+    P = qp.Field2d(ctx, 1, 0)
+    P.set_rs(psi)
+    sp.extpsi(P, ctx.dex)
+    gp, gk = sp.get_particles(pp.shape[1])
+    O.extpsi(pp, kp, psi, -1.0, ctx.dex, ix, iy)
+    assert np.array_equal(gk, kp)
+    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=1e-6)
+
+
+def test_amjdp(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 13), ix, iy)
+    fxy, bxy, psit = _fields(O, ctx, 40)
+    sp = _species_with(qp, ctx, pp, kp)
+    F, B, P = _upload_fields(qp, ctx, fxy, bxy, psit)
+    cu, dcu, amu = qp.Field2d(ctx, 3, 0), qp.Field2d(ctx, 2, 0), qp.Field2d(ctx, 3, 0)
+    for f in (cu, dcu, amu):
+        f.as_(0.0)
+    dex, dt = ctx.dex, ctx.dxi
+    sp.amjdp(F, B, P, cu, amu, dcu, dex)
+    ocu, odcu, oamu = O.rs_zeros(3, ix, iy), O.rs_zeros(2, ix, iy), O.rs_zeros(3, ix, iy)
+    O.amjdp(pp, kp, fxy, bxy, psit, ocu, odcu, oamu, -1.0, dt, dex, ix, iy)
+    for a in (ocu, odcu, oamu):
+        O.acguard(a, ix, iy)
+    assert rel_l2(cu.get_rs(), ocu) < 1e-5
+    assert rel_l2(dcu.get_rs(), odcu) < 1e-5
+    assert rel_l2(amu.get_rs(), oamu) < 1e-5
+    gp, gk = sp.get_particles(pp.shape[1])
+    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=1e-6)
+
+
+def test_partpush_then_pmove(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 14, pscale=0.5), ix, iy, xtras=0.5)
+    fxy, bxy, psit = _fields(O, ctx, 50, amp=3.0)
+    sp = _species_with(qp, ctx, pp, kp)
+    F, B, P = _upload_fields(qp, ctx, fxy, bxy, psit)
+    dex = ctx.dex
+    sp.partpush(F, B, P, dex)
+    gp, gk = sp.get_particles(pp.shape[1])
+    ncl, ihole, ntmax = O.push(pp, kp, fxy, bxy, psit, -1.0, ctx.dxi, dex, ix, iy)
+    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=2e-6)
+    # re-binning from identical post-push data must agree bit for bit, tile by tile
+    sp.set_particles(pp, kp)
+    sp.pmove()
+    gp2, gk2 = sp.get_particles(max(sp.nppmx, pp.shape[1]))
+    rc = O.pmove(pp, kp, ncl, ihole, ntmax, ix, iy)
+    assert rc == 0
+    assert np.array_equal(gk2, kp)
+    for t in range(len(kp)):
+        a = gp2[:, : kp[t], t]
+        b = pp[:, : kp[t], t]
+        ka, kb = np.lexsort(a[::-1]), np.lexsort(b[::-1])
+        assert np.array_equal(a[:, ka], b[:, kb]), t
+    assert O.check_tiles(np.asfortranarray(gp2), gk2, ix, iy) == 0
+
+
+def test_fused_push_equals_partpush_pmove(qp, ctx, oracle_mod):
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 15, pscale=0.5), ix, iy, xtras=0.5)
+    fxy, bxy, psit = _fields(O, ctx, 60, amp=3.0)
+    F, B, P = _upload_fields(qp, ctx, fxy, bxy, psit)
+    s1 = _species_with(qp, ctx, pp, kp)
+    s1.push(F, B, P, ctx.dex)
+    s2 = _species_with(qp, ctx, pp, kp)
+    s2.partpush(F, B, P, ctx.dex)
+    s2.pmove()
+    a, ka = s1.get_particles(max(s1.nppmx, s2.nppmx))
+    b, kb = s2.get_particles(max(s1.nppmx, s2.nppmx))
+    assert np.array_equal(ka, kb)
+    assert np.array_equal(a, b)
+
+
+def test_push_overflow_recovers(qp, oracle_mod):
+    """Tiny tile capacity forces the grow-and-retry path of pmove."""
+    O = oracle_mod
+    c = qp.Context(6, 6, 4, [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]])
+    sp = qp.Species2d(c, ppc=(2, 2), xtras=0.01)
+    pp, kp = sp.get_particles()
+    n0 = kp.sum()
+    fxy, bxy, psit = _fields(O, c, 70, amp=0.0)
+    # a radial inward kick concentrates particles into the central tiles
+    F, B, P = _upload_fields(qp, c, fxy, bxy, psit)
+    nx = 64
+    x = pp[0] - nx / 2
+    y = pp[1] - nx / 2
+    pp[2] = -0.6 * x
+    pp[3] = -0.6 * y
+    sp.set_particles(pp, kp)
+    cap0 = sp.nppmx
+    sp.push(F, B, P, c.dex)
+    gp, gk = sp.get_particles()
+    assert gk.sum() == n0
+    assert sp.nppmx > cap0
+    assert O.check_tiles(np.asfortranarray(gp), gk, 6, 6) == 0
+    c.close()
+
+
+def test_beam_loader_and_deposit(qp, ctx, oracle_mod):
+    O = oracle_mod
+    cfg = make_config(ind=(ctx.indx, ctx.indy, ctx.indz))
+    b = cfg["beams"][0]
+    bm = qp.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
+                   peak_density=b["peak_density"], quiet_start=True, center=b["center"],
+                   sigma=b["sigma"], sigma_v=b["sigma_v"])
+    osim = O.Sim(cfg, np.float32)
+    ref = osim.get("beam0").reshape(7, -1, order="F")
+    got = bm.get_particles()
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
+    bm.qdp()
+    osim.begin3d()
+    q3 = bm.get_q3d()
+    oq = osim.get("q3d").reshape(q3.shape, order="F")
+    assert rel_l2(q3, oq) < 1e-6
+    bm.close()
+
+
+def _gpu_sim(qp, cfg, use_graphs=True):
+    ind = cfg["grid"]["ind"]
+    c = qp.Context(ind[0], ind[1], ind[2], cfg["grid"]["box"])
+    s = cfg["species"]
+    sp = qp.Species2d(c, ppc=tuple(s["ppc"]), q=s["q"], m=s["m"], density=s["density"],
+                      xtras=s["xtras"])
+    beams = []
+    for b in cfg["beams"]:
+        beams.append(qp.Beam3d(c, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
+                               peak_density=b["peak_density"], quiet_start=b["quiet_start"],
+                               center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
+    sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs)
+    return c, sp, beams, sim
+
+
+def test_uniform_plasma_stays_zero_on_gpu(qp):
+    cfg = make_config(ind=(6, 6, 4), beams=[])
+    c, sp, beams, sim = _gpu_sim(qp, cfg)
+    pp0, kp0 = sp.get_particles()
+    sim.step3d()
+    for name in ("psi", "fxy", "bxyz", "psit", "cu"):
+        assert np.all(sim.get_field(name) == 0), name
+    assert np.all(sim.get_3d("bexyz") == 0)
+    sim.close()
+    c.close()
+
+
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_full_3d_step_matches_oracle(qp, oracle_mod, use_graphs):
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 5), iter=2)
+    c, sp, beams, sim = _gpu_sim(qp, cfg, use_graphs)
+    st = sim.step3d()
+    assert st.slices == 32
+    o32 = O.Sim(cfg, np.float32)
+    o64 = O.Sim(cfg, np.float64)
+    o32.begin3d()
+    o64.begin3d()
+    for j in range(1, 33):
+        o32.slice(j)
+        o64.slice(j)
+    be = sim.get_3d("bexyz")
+    bb = sim.get_3d("bbxyz")
+    ob32 = o32.get("bexyz").reshape(be.shape, order="F")
+    ob64 = o64.get("bexyz").reshape(be.shape, order="F")
+    bb64 = o64.get("bbxyz").reshape(bb.shape, order="F")
+    e_gpu = rel_l2(be, ob64)
+    e_ref = rel_l2(ob32, ob64)
+    assert e_gpu < 1e-4, (e_gpu, e_ref)
+    assert rel_l2(bb, bb64) < 1e-3
+    q3 = sim.get_3d("q3")
+    oq3 = o64.get("q3").reshape(q3.shape, order="F")
+    assert rel_l2(q3, oq3) < 1e-4
+    for name in ("psit", "bxyz"):
+        assert rel_l2(sim.get_field(name), o64.get(name).reshape(sim.get_field(name).shape,
+                                                                 order="F")) < 1e-3, name
+    sim.close()
+    c.close()

@@ -1,0 +1,208 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+QuickPIC has no tests or golden outputs of its own, so the oracle's
+restatement is pinned here by independent answers: exact-integer ranorm draws,
+scipy's DST-I/DCT-I, closed-form Poisson eigenmodes, charge conservation of the
+deposit, invariants of the push, and the cold uniform plasma that must stay
+exactly unperturbed without a beam.
+"""
+import os
+
+import numpy as np
+import pytest
+from conftest import make_config, rel_l2
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_ranorm_matches_exact_integer_generator(oracle_mod):
+    O = oracle_mod
+    gold = np.load(os.path.join(GOLD, "ranorm.npz"))["draws"]
+    O.ranorm_reset()
+    got = np.array([O.ranorm() for _ in range(len(gold))])
+    assert np.array_equal(got, gold)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 2e-5)])
+def test_nr_lines_are_dst1_dct1(oracle_mod, dtype, tol):
+    """x/y passes of fft2d_lib77.f: isign=+1 is the unnormalised DST-I/DCT-I,
+    isign=-1 is the same scaled by 0.5/(nx*ny) (x) or 0.5 (y)."""
+    O = oracle_mod
+    g = np.load(os.path.join(GOLD, "sincos.npz"))
+    for ind, x, s, c in zip(g["ind"], g["x"], g["sine"], g["cosine"]):
+        n = 1 << int(ind)
+        for parity, ref in ((0, s[: n + 1]), (1, c[: n + 1])):
+            for xpass, isign, scale in ((1, 1, 1.0), (0, 1, 1.0), (1, -1, 0.5 / (n * n)),
+                                        (0, -1, 0.5)):
+                v = np.zeros(n + 2, dtype=dtype)
+                v[: n + 1] = x[: n + 1]
+                O.line(v, parity, xpass, isign, int(ind), int(ind))
+                assert rel_l2(v[: n + 1], scale * ref) < tol, (ind, parity, xpass, isign)
+
+
+@pytest.mark.parametrize("kind,dim", [(1, 1), (2, 1), (1, 2), (2, 2), (1, 3), (2, 3), (3, 3)])
+def test_fft_roundtrip_and_guard(oracle_mod, kind, dim):
+    O = oracle_mod
+    ix, iy = 5, 4
+    nx, ny = 1 << ix, 1 << iy
+    rng = np.random.default_rng(kind * 10 + dim)
+    rs = O.rs_zeros(dim, ix, iy, np.float64)
+    rs[:, : nx + 1, : ny + 1] = rng.standard_normal((dim, nx + 1, ny + 1))
+    orig = rs.copy()
+    ks = O.ks_zeros(dim, ix, iy, np.float64)
+    O.fftrk(rs, ks, kind, ix, iy)
+    O.fftkr(rs, ks, kind, ix, iy)
+    par = {(1, 1): [(0, 0)], (2, 1): [(1, 1)], (1, 2): [(1, 0), (0, 1)], (2, 2): [(0, 1), (1, 0)],
+           (1, 3): [(1, 0), (0, 1), (0, 0)], (2, 3): [(0, 1), (1, 0), (1, 1)],
+           (3, 3): [(0, 0), (0, 0), (1, 1)]}[(kind, dim)]
+    for c, (px, py) in enumerate(par):
+        exp = orig[c, : nx + 1, : ny + 1].copy()
+        if px == 0:
+            exp[0, :] = 0
+            exp[nx, :] = 0
+        if py == 0:
+            exp[:, 0] = 0
+            exp[:, ny] = 0
+        got = rs[c, : nx + 1, : ny + 1]
+        assert np.allclose(got[:, :ny], exp[:, :ny], atol=1e-12)
+        # copyguard: row ny is a copy of row 0 after fftkr
+        assert np.array_equal(rs[c, :, ny], rs[c, :, 0])
+
+
+def test_poisson_eigenmode(oracle_mod):
+    """pot of the (a, b) sine mode is Re(ffc) times that mode (MPPOTPD2)."""
+    O = oracle_mod
+    ix = iy = 5
+    n = 1 << ix
+    a, b = 3, 5
+    x = np.arange(n + 2)[:, None]
+    y = np.arange(2 * n + 1)[None, :]
+    q = O.rs_zeros(1, ix, iy, np.float64)
+    q[0] = np.sin(np.pi * a * x / n) * np.sin(np.pi * b * y / n)
+    q[0, :, n + 1:] = 0
+    ks = O.ks_zeros(1, ix, iy, np.float64)
+    O.fftrk(q, ks, 1, ix, iy)
+    # DST-I maps sin(pi a j / n) to n at mode a; the forward 2D transform is
+    # 0.25/(nx*ny) times DST-I in x and y, so the mode's coefficient is 1/4
+    expect = np.zeros_like(ks)
+    expect[0, b, a] = 0.25
+    assert np.allclose(ks, expect, atol=1e-12)
+    t = O.ffc(ix, iy, np.float64)
+    pk = O.ks_zeros(1, ix, iy, np.float64)
+    O.pot(ks, pk, t, ix, iy)
+    assert np.isclose(pk[0, b, a], t[0, b, a] * ks[0, b, a])
+    rest = pk.copy()
+    rest[0, b, a] = 0
+    assert np.abs(rest).max() < 1e-14
+
+
+def test_deposit_conserves_charge(oracle_mod):
+    O = oracle_mod
+    ix = iy = 6
+    part = O.dist2d_000(ix, iy, 2, 2, dtype=np.float64)
+    rng = np.random.default_rng(1)
+    part[0] += rng.uniform(-0.24, 0.24, part.shape[1])
+    part[1] += rng.uniform(-0.24, 0.24, part.shape[1])
+    pp, kp, _ = O.bin_particles(part, ix, iy)
+    assert O.check_tiles(pp, kp, ix, iy) == 0
+    q = O.rs_zeros(1, ix, iy, np.float64)
+    O.qdeposit(pp, kp, q, ix, iy)
+    O.acguard(q, ix, iy)
+    assert np.isclose(q.sum(), part[7].sum(), rtol=1e-12)
+    assert np.all(q[0, :, (1 << iy):] == 0)
+
+
+def test_push_rotation_preserves_pperp(oracle_mod):
+    """With E = 0 and a uniform Bz the push only rotates p_perp."""
+    O = oracle_mod
+    ix = iy = 5
+    part = O.dist2d_000(ix, iy, 1, 1, dtype=np.float64)
+    rng = np.random.default_rng(2)
+    part[2] = rng.normal(0, 0.1, part.shape[1])
+    part[3] = rng.normal(0, 0.1, part.shape[1])
+    pp, kp, _ = O.bin_particles(part, ix, iy)
+    fxy = O.rs_zeros(2, ix, iy, np.float64)
+    bxy = O.rs_zeros(3, ix, iy, np.float64)
+    bxy[2] = 0.7
+    psit = O.rs_zeros(1, ix, iy, np.float64)
+    before = []
+    for t in range(pp.shape[2]):
+        before.append(np.hypot(pp[2, : kp[t], t], pp[3, : kp[t], t]))
+    O.push(pp, kp, fxy, bxy, psit, -1.0, 0.1, 0.2, ix, iy)
+    for t in range(pp.shape[2]):
+        after = np.hypot(pp[2, : kp[t], t], pp[3, : kp[t], t])
+        assert np.allclose(after, before[t], rtol=1e-13)
+
+
+def test_push_pmove_keeps_every_particle(oracle_mod):
+    O = oracle_mod
+    ix = iy = 6
+    part = O.dist2d_000(ix, iy, 2, 2, dtype=np.float64)
+    pp, kp, nppmx = O.bin_particles(part, ix, iy, xtras=0.5)
+    rng = np.random.default_rng(3)
+    fxy = O.rs_zeros(2, ix, iy, np.float64)
+    fxy[:, :, :65] = rng.normal(0, 3.0, (2, 66, 65))
+    bxy = O.rs_zeros(3, ix, iy, np.float64)
+    psit = O.rs_zeros(1, ix, iy, np.float64)
+    n0 = kp.sum()
+    ncl, ihole, ntmax = O.push(pp, kp, fxy, bxy, psit, -1.0, 0.1, 0.2, ix, iy)
+    moved = np.concatenate([pp[:, : kp[t], t] for t in range(len(kp))], axis=1)
+    rc = O.pmove(pp, kp, ncl, ihole, ntmax, ix, iy)
+    assert rc == 0
+    assert kp.sum() == n0
+    assert O.check_tiles(pp, kp, ix, iy) == 0
+    after = np.concatenate([pp[:, : kp[t], t] for t in range(len(kp))], axis=1)
+    nx = float(1 << ix)
+    w = moved.copy()
+    w[0] = np.where(w[0] < 0, w[0] + nx, w[0])
+    w[0] = np.where(w[0] >= nx, w[0] - nx, w[0])
+    w[1] = np.where(w[1] < 0, w[1] + nx, w[1])
+    w[1] = np.where(w[1] >= nx, w[1] - nx, w[1])
+    key = lambda a: np.lexsort(a[::-1])
+    assert np.array_equal(w[:, key(w)], after[:, key(after)])
+
+
+def test_uniform_plasma_without_beam_stays_unperturbed(oracle_mod):
+    O = oracle_mod
+    cfg = make_config(ind=(5, 5, 3), beams=[])
+    sim = O.Sim(cfg, np.float32)
+    pp0 = sim.get("ppart").copy()
+    sim.begin3d()
+    for j in range(1, 5):
+        sim.slice(j)
+    for name in ("psi", "fxy", "bxyz", "psit", "cu", "epw_k"):
+        assert np.all(sim.get(name) == 0), name
+    assert np.array_equal(sim.get("ppart"), pp0)
+
+
+def test_beam_charge_normalisation(oracle_mod):
+    """The deposited beam charge equals np * qm and peaks near peak_density."""
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 6))
+    sim = O.Sim(cfg, np.float64)
+    sim.begin3d()
+    q3 = sim.get("q3d")
+    bm = sim.get("beam0").reshape(7, -1, order="F")
+    assert np.isclose(q3.sum(), bm[6].sum(), rtol=1e-12)
+    # a quiet-start beam is symmetric about its centre in x and y
+    x0 = (0.0 + 6.0) / (12.0 / 64)
+    assert abs(bm[0].mean() - x0) < 1e-9
+
+
+def test_fp32_oracle_tracks_fp64(oracle_mod):
+    """The SGL restatement stays within FP32 roundoff of the DBL one for a few slices."""
+    O = oracle_mod
+    cfg = make_config(ind=(5, 5, 4), beams=[dict(np=[16, 16, 32], q=-1.0, m=1.0, gamma=20000.0,
+                                                peak_density=2.0, quiet_start=True,
+                                                center=[0.0, 0.0, 2.5], sigma=[0.6, 0.6, 0.5],
+                                                sigma_v=[0.0, 0.0, 0.0])])
+    s32, s64 = O.Sim(cfg, np.float32), O.Sim(cfg, np.float64)
+    s32.begin3d()
+    s64.begin3d()
+    for j in range(1, 9):
+        s32.slice(j)
+        s64.slice(j)
+    for name in ("psi", "fxy", "bxyz", "psit", "cu"):
+        e = rel_l2(s32.get(name), s64.get(name))
+        assert e < 1e-4, (name, e)
+    assert np.abs(s64.get("psi")).max() > 1e-3  # the beam drove a wake
