@@ -54,7 +54,11 @@ def _ctype(dtype):
 
 
 def _p(a: np.ndarray):
-    assert a.flags["F_CONTIGUOUS"] or a.flags["C_CONTIGUOUS"]
+    # every multi-dimensional array is a Fortran-layout reference array
+    if a.ndim > 1 and not a.flags["F_CONTIGUOUS"]:
+        raise ValueError("oracle arrays must be Fortran-contiguous (reference layout)")
+    if not a.flags["F_CONTIGUOUS"]:
+        raise ValueError("oracle arrays must be contiguous")
     return a.ctypes.data_as(C.c_void_p)
 
 

@@ -4,8 +4,9 @@ Every test feeds the engine (through the C ABI) and the oracle the same inputs
 in the reference's layouts.  Tolerances (relative L2 unless stated):
   * transforms and Fourier-space solves: 2e-5 against the FP32 oracle (whose own
     NR transforms carry ~5e-6 of FP32 roundoff) and 1e-5 against the FP64 oracle;
-  * particle kernels: per particle, 2e-6 relative / 1e-6 absolute (FMA contraction
-    on the GPU is the only difference in the arithmetic);
+  * Fourier-space solves and per-particle results (extpsi, the push, the p6
+    update of amjdp): bit-exact (those kernels are built without FMA
+    contraction and follow the reference's operation order);
   * deposits: 1e-6 (shared-memory and edge atomics change the summation order);
   * re-binning: bit-exact per tile (it only moves data);
   * whole slices: 1e-4 on fields after several slices (the roundoff above feeds
@@ -55,7 +56,7 @@ def test_fftrk_fftkr(qp, ctx, oracle_mod, kind, dim):
     f.fftrk(kind)
     gk = f.get_ks()
     ks32 = O.ks_zeros(dim, ix, iy, np.float32)
-    r32 = rs.copy()
+    r32 = rs.copy(order="F")
     O.fftrk(r32, ks32, kind, ix, iy)
     ks64 = O.ks_zeros(dim, ix, iy, np.float64)
     r64 = rs.astype(np.float64)
@@ -66,7 +67,7 @@ def test_fftrk_fftkr(qp, ctx, oracle_mod, kind, dim):
     f.set_ks(ks64.astype(np.float32))
     f.fftkr(kind)
     gr = f.get_rs()
-    k64 = ks64.copy()
+    k64 = ks64.copy(order="F")
     O.fftkr(r64, k64, kind, ix, iy)
     ny = 1 << iy
     assert rel_l2(gr[:, :, : ny + 1], r64[:, :, : ny + 1]) < TOL_FFT64
@@ -118,7 +119,7 @@ def test_kspace_solves(qp, ctx, oracle_mod):
         exp = O.ks_zeros(dim, ix, iy, np.float32)
         ref(exp)
         got = dst.get_ks()
-        assert np.allclose(got, exp, rtol=2e-6, atol=1e-7), name
+        assert np.array_equal(got, exp), name
     # bfqp: the transverse-B corrector (dcu modified in place)
     dcu = _rand_ks(O, 2, ix, iy, 3)
     amu = _rand_ks(O, 3, ix, iy, 4)
@@ -129,10 +130,10 @@ def test_kspace_solves(qp, ctx, oracle_mod):
     fb.set_ks(bxy)
     dex = ctx.dex
     fcu.bfqp(fd, fa, fb, dex * dex, dex)
-    d_ref, b_ref = np.asfortranarray(dcu.copy()), np.asfortranarray(bxy.copy())
+    d_ref, b_ref = np.asfortranarray(dcu), np.asfortranarray(bxy)
     O.bfqp(np.asfortranarray(cu), d_ref, np.asfortranarray(amu), b_ref, t, dex * dex, dex, ix, iy)
-    assert np.allclose(fd.get_ks(), d_ref, rtol=2e-6, atol=1e-6)
-    assert np.allclose(fb.get_ks(), b_ref, rtol=2e-6, atol=1e-6)
+    assert np.array_equal(fd.get_ks(), d_ref)
+    assert np.array_equal(fb.get_ks(), b_ref)
 
 
 def _particles(O, ix, iy, seed, jitter=0.2, pscale=0.05):
@@ -193,8 +194,9 @@ def test_charge_deposit(qp, ctx, oracle_mod):
     exp = q + sp.get_qn()
     got = qe.get_rs()
     assert rel_l2(got, exp) < 1e-6
-    assert np.isclose(got.sum(), (pp[7] * (np.arange(pp.shape[1])[:, None] < kp[None, :])).sum()
-                      + sp.get_qn().sum(), rtol=1e-5)
+    live = np.arange(pp.shape[1])[:, None] < kp[None, :]
+    total = float((pp[7] * live).sum()) + float(sp.get_qn().sum())
+    assert abs(float(got.sum()) - total) < 1e-3
 
 
 def test_extpsi(qp, ctx, oracle_mod):
@@ -209,7 +211,7 @@ def test_extpsi(qp, ctx, oracle_mod):
     gp, gk = sp.get_particles(pp.shape[1])
     O.extpsi(pp, kp, psi, -1.0, ctx.dex, ix, iy)
     assert np.array_equal(gk, kp)
-    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=1e-6)
+    assert np.array_equal(_flat(gp, gk), _flat(pp, kp))
 
 
 def test_amjdp(qp, ctx, oracle_mod):
@@ -232,7 +234,7 @@ def test_amjdp(qp, ctx, oracle_mod):
     assert rel_l2(dcu.get_rs(), odcu) < 1e-5
     assert rel_l2(amu.get_rs(), oamu) < 1e-5
     gp, gk = sp.get_particles(pp.shape[1])
-    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=1e-6)
+    assert np.array_equal(_flat(gp, gk), _flat(pp, kp))
 
 
 def test_partpush_then_pmove(qp, ctx, oracle_mod):
@@ -246,7 +248,7 @@ def test_partpush_then_pmove(qp, ctx, oracle_mod):
     sp.partpush(F, B, P, dex)
     gp, gk = sp.get_particles(pp.shape[1])
     ncl, ihole, ntmax = O.push(pp, kp, fxy, bxy, psit, -1.0, ctx.dxi, dex, ix, iy)
-    assert np.allclose(_flat(gp, gk), _flat(pp, kp), rtol=2e-6, atol=2e-6)
+    assert np.array_equal(_flat(gp, gk), _flat(pp, kp))
     # re-binning from identical post-push data must agree bit for bit, tile by tile
     sp.set_particles(pp, kp)
     sp.pmove()
@@ -339,14 +341,18 @@ def _gpu_sim(qp, cfg, use_graphs=True):
     return c, sp, beams, sim
 
 
-def test_uniform_plasma_stays_zero_on_gpu(qp):
+def test_uniform_plasma_stays_unperturbed_on_gpu(qp):
+    """Without a beam the species charge cancels its ion background.  The
+    reference does this exactly with one thread; the GPU deposit (like the
+    reference's OpenMP edge atomics) sums in a nondeterministic order, so the
+    residue is FP32 roundoff of the O(1) density, and the fields it drives stay
+    at that level."""
     cfg = make_config(ind=(6, 6, 4), beams=[])
     c, sp, beams, sim = _gpu_sim(qp, cfg)
-    pp0, kp0 = sp.get_particles()
     sim.step3d()
     for name in ("psi", "fxy", "bxyz", "psit", "cu"):
-        assert np.all(sim.get_field(name) == 0), name
-    assert np.all(sim.get_3d("bexyz") == 0)
+        assert np.abs(sim.get_field(name)).max() < 1e-5, name
+    assert np.abs(sim.get_3d("bexyz")).max() < 1e-5
     sim.close()
     c.close()
 
