@@ -21,6 +21,7 @@
 #include "qp_loader.h"
 #include "qp_misc.cuh"
 #include "qp_part.cuh"
+#include "qp_slice.cuh"
 
 using namespace qp;
 
@@ -156,7 +157,8 @@ extern "C" int qp_ctx_create(const qp_grid_desc* grid, int device, qp_ctx** out)
   ctx->dy = (float)((float)(grid->box[1][1]) - (float)(grid->box[1][0])) / (float)ctx->g.ny;
   ctx->dxi = (float)((float)(grid->box[2][1]) - (float)(grid->box[2][0])) / (float)ctx->nz;
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-  if (fft_kernels_init() || part_kernels_init()) return fail(ctx, __LINE__, "kernel init failed");
+  if (fft_kernels_init() || part_kernels_init() || slice_kernels_init())
+    return fail(ctx, __LINE__, "kernel init failed");
   if (line_tables_build(&ctx->tx, grid->indx)) return fail(ctx, __LINE__, "table alloc failed");
   if (grid->indy == grid->indx)
     ctx->ty = ctx->tx;
@@ -575,7 +577,10 @@ extern "C" int qp_field2d_ag(qp_field2d* f) {
 }
 
 // --------------------------------------------------------------- species
+// Tile capacities are rounded up to a multiple of 4 so every tile segment
+// starts on a 16-byte boundary (the particle kernels use float4 accesses).
 static int part_alloc(PartBuf* P, int ntiles, int cap) {
+  cap = (cap + 3) & ~3;
   P->cap = cap;
   for (int c = 0; c < NCOMP; ++c) {
     P->c[c] = dalloc((size_t)ntiles * cap);
@@ -676,10 +681,11 @@ extern "C" int qp_species_create(qp_ctx* ctx, const qp_species_desc* d, float s,
   for (int v : cnt) nppmx = std::max(nppmx, v);
   const float xtras = d->xtras > 0 ? d->xtras : 0.2f;
   sp->nppmx0 = (int)((1.0f + xtras) * (float)nppmx);
-  const int cap = std::max(sp->nppmx0, 1);
-  if (part_alloc(&sp->A, tg.ntiles, cap) || part_alloc(&sp->B, tg.ntiles, cap) ||
-      part_alloc(&sp->P0, tg.ntiles, cap))
+  if (part_alloc(&sp->A, tg.ntiles, std::max(sp->nppmx0, 1)) ||
+      part_alloc(&sp->B, tg.ntiles, std::max(sp->nppmx0, 1)) ||
+      part_alloc(&sp->P0, tg.ntiles, std::max(sp->nppmx0, 1)))
     return fail(ctx, __LINE__, "out of device memory (particles)");
+  const int cap = sp->P0.cap;  // rounded up to a multiple of 4 by part_alloc
   const int capin = std::max(64, (int)(xtras * (float)nppmx));
   if (inbox_alloc(&sp->ib, tg.ntiles, capin)) return fail(ctx, __LINE__, "out of device memory");
   {

@@ -58,7 +58,7 @@ struct DevStatus {
   int need_inbox;     // movers a tile must accept
   int cursor;         // slice cursor of the fused 3D step
   int iter_done;      // iterations run in the current slice
-  int pad[2];
+  int pad[2];         // pad[0]: CTA completion counter of the store kernel
   float resid_num;    // convergence residual accumulators
   float resid_den;
 };

@@ -123,6 +123,11 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
       if (lane == 0) dg[n + 1] = d[n + 1];
     }
   }
+  for (int z = blockIdx.y; z < job.nzero; z += job.ncomp) {
+    float* p = job.zero[z] + (long long)y0 * g.rp;
+    const int rows = min(8, g.ny + 1 - y0);
+    for (int i = threadIdx.x; i < rows * g.rp; i += 256) p[i] = 0.f;
+  }
 }
 
 // ------------------------------------------------------------------ y pass

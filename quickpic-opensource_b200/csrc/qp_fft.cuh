@@ -31,6 +31,10 @@ struct XComp {
 struct XJob {
   XComp c[QP_MAX_JOB];
   int ncomp;
+  // xinv only: real-space planes whose rows this launch clears (plane i is
+  // cleared by the CTAs of component i % ncomp)
+  float* zero[8];
+  int nzero;
 };
 
 struct YComp {

@@ -95,7 +95,7 @@ __device__ __forceinline__ float2* warp_cfft(float2* a, float2* b, int logN, con
 
 // Unnormalised DST-I (parity 0) or DCT-I (parity 1) of L[0..n], in place.
 // L and S are per-warp shared buffers of at least n + 4 floats, 8-byte aligned.
-__device__ __noinline__ void warp_line_transform(float* L, float* S, int logn, int parity,
+static __device__ __noinline__ void warp_line_transform(float* L, float* S, int logn, int parity,
                                                  const LineTables& t, int lane) {
   const int n = 1 << logn;
   const int h = n >> 1;

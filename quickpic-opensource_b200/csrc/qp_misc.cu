@@ -161,7 +161,7 @@ __global__ void k_kscale(GridDims g, float* p, float v, const DevStatus* st) {
 // updated in place as in the reference.
 __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by, const float* bz,
                           const float* psit, Planes3 be, Planes3 bb, float dex, int store,
-                          const DevStatus* st) {
+                          float* zero_q, DevStatus* st) {
   if (st->error) return;
   const long long n = g.rplane;
   const long long pl = (long long)st->cursor * g.rplane;
@@ -184,6 +184,18 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
       bb.p[0][pl + i] = b1;
       bb.p[1][pl + i] = b2;
       bb.p[2][pl + i] = bz[i];
+    }
+    if (zero_q) zero_q[i] = 0.f;  // species charge plane, ready for the next deposit
+  }
+  // the last CTA to finish advances the slice cursor
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int done = atomicAdd(&st->pad[0], 1);
+    if (done == (int)gridDim.x - 1) {
+      st->pad[0] = 0;
+      st->cursor = st->cursor + 1;
+      __threadfence();
     }
   }
 }
@@ -244,12 +256,12 @@ void launch_kscale(const GridDims& g, float* p, float v, const DevStatus* st, cu
 void launch_cursor(DevStatus* st, int v, cudaStream_t s) { k_cursor<<<1, 1, 0, s>>>(st, v); }
 
 void launch_store3d(const GridDims& g, float* const* fxy, float* const* bxyz, const float* psit,
-                    const Planes3& be, const Planes3& bb, float dex, int store,
-                    const DevStatus* st, cudaStream_t s) {
+                    const Planes3& be, const Planes3& bb, float dex, int store, float* zero_q,
+                    DevStatus* st, cudaStream_t s) {
   long long blocks = (g.rplane + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_store3d<<<(int)blocks, 256, 0, s>>>(g, fxy[0], fxy[1], bxyz[0], bxyz[1], bxyz[2], psit, be,
-                                        bb, dex, store, st);
+                                        bb, dex, store, zero_q, st);
 }
 
 }  // namespace qp

@@ -58,6 +58,9 @@ __device__ __forceinline__ void flush(const float* s, float* plane, const TileGe
   }
 }
 
+// Charge deposit with the run scheme of k_amjdp: 4 consecutive particles per
+// thread, corner weights of a run of particles in one cell summed in
+// registers before the shared-memory atomics.
 __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, float* q,
                                                      DevStatus* st) {
   __shared__ float sq[TN * TN];
@@ -69,23 +72,56 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
   __syncthreads();
   const int n = P.count[t];
   const long long base = (long long)t * P.cap;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const float x = P.c[0][base + k], y = P.c[1][base + k], qm = P.c[7][base + k];
-    int nn = (int)x, mm = (int)y;
-    const float dxp = qm * (x - (float)nn);
-    const float dyp = y - (float)mm;
-    nn -= noffp;
-    mm -= moffp;
-    if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
-      raise_error(st, -3);
-      continue;
+  for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
+    const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
+    const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + base + k0);
+    const float4 QM = *reinterpret_cast<const float4*>(P.c[7] + base + k0);
+    const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
+    const float qs[4] = {QM.x, QM.y, QM.z, QM.w};
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    int cell = -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (k0 + j < n) {
+        const float x = xs[j], y = ys[j], qm = qs[j];
+        int nn = (int)x, mm = (int)y;
+        const float dxp = qm * (x - (float)nn);
+        const float dyp = y - (float)mm;
+        nn -= noffp;
+        mm -= moffp;
+        if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
+          raise_error(st, -3);
+          continue;
+        }
+        const float amx = qm - dxp, amy = 1.f - dyp;
+        const float w0 = amx * amy, w1 = dxp * amy, w2 = amx * dyp, w3 = dxp * dyp;
+        const int c = mm * TN + nn;
+        if (c != cell) {
+          if (cell >= 0) {
+            atomicAdd(sq + cell, acc[0]);
+            atomicAdd(sq + cell + 1, acc[1]);
+            atomicAdd(sq + cell + TN, acc[2]);
+            atomicAdd(sq + cell + TN + 1, acc[3]);
+          }
+          cell = c;
+          acc[0] = w0;
+          acc[1] = w1;
+          acc[2] = w2;
+          acc[3] = w3;
+        } else {
+          acc[0] += w0;
+          acc[1] += w1;
+          acc[2] += w2;
+          acc[3] += w3;
+        }
+      }
     }
-    const float amx = qm - dxp, amy = 1.f - dyp;
-    float* s = sq + mm * TN + nn;
-    atomicAdd(s, amx * amy);
-    atomicAdd(s + 1, dxp * amy);
-    atomicAdd(s + TN, amx * dyp);
-    atomicAdd(s + TN + 1, dxp * dyp);
+    if (cell >= 0) {
+      atomicAdd(sq + cell, acc[0]);
+      atomicAdd(sq + cell + 1, acc[1]);
+      atomicAdd(sq + cell + TN, acc[2]);
+      atomicAdd(sq + cell + TN + 1, acc[3]);
+    }
   }
   __syncthreads();
   flush(sq, q, tg, noffp, moffp, 1.f);
@@ -103,27 +139,41 @@ __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const fl
   const float dx2 = dex * dex;
   const int n = P.count[t];
   const long long base = (long long)t * P.cap;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const float x = P.c[0][base + k], y = P.c[1][base + k];
-    const float vx = P.c[2][base + k], vy = P.c[3][base + k];
-    int nn = (int)x, mm = (int)y;
-    const float dxp = x - (float)nn, dyp = y - (float)mm;
-    nn -= noffp;
-    mm -= moffp;
-    if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
-      raise_error(st, -3);
-      continue;
+  for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
+    const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
+    const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + base + k0);
+    const float4 VX = *reinterpret_cast<const float4*>(P.c[2] + base + k0);
+    const float4 VY = *reinterpret_cast<const float4*>(P.c[3] + base + k0);
+    float4 P6 = *reinterpret_cast<const float4*>(P.c[5] + base + k0);
+    float4 P7 = *reinterpret_cast<const float4*>(P.c[6] + base + k0);
+    const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
+    const float vxs[4] = {VX.x, VX.y, VX.z, VX.w}, vys[4] = {VY.x, VY.y, VY.z, VY.w};
+    float p6[4] = {P6.x, P6.y, P6.z, P6.w}, p7[4] = {P7.x, P7.y, P7.z, P7.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (k0 + j < n) {
+        const float x = xs[j], y = ys[j], vx = vxs[j], vy = vys[j];
+        int nn = (int)x, mm = (int)y;
+        const float dxp = x - (float)nn, dyp = y - (float)mm;
+        nn -= noffp;
+        mm -= moffp;
+        if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
+          raise_error(st, -3);
+          continue;
+        }
+        const float amx = 1.f - dxp, amy = 1.f - dyp;
+        const float* s = sp + mm * TN + nn;
+        float dx = amx * s[0];
+        dx = amy * (dxp * s[1] + dx);
+        const float acx = amx * s[TN];
+        dx = dx + dyp * (dxp * s[TN + 1] + acx);
+        dx = -dx * dx2 * qbm;
+        p7[j] = 1.f + dx;
+        p6[j] = dx + (dx2 * (vx * vx + vy * vy) - dx * dx - 2.f * dx) / (2.f * (1.f + dx)) + 1.f;
+      }
     }
-    const float amx = 1.f - dxp, amy = 1.f - dyp;
-    const float* s = sp + mm * TN + nn;
-    float dx = amx * s[0];
-    dx = amy * (dxp * s[1] + dx);
-    const float acx = amx * s[TN];
-    dx = dx + dyp * (dxp * s[TN + 1] + acx);
-    dx = -dx * dx2 * qbm;
-    P.c[6][base + k] = 1.f + dx;
-    P.c[5][base + k] =
-        dx + (dx2 * (vx * vx + vy * vy) - dx * dx - 2.f * dx) / (2.f * (1.f + dx)) + 1.f;
+    *reinterpret_cast<float4*>(P.c[5] + base + k0) = make_float4(p6[0], p6[1], p6[2], p6[3]);
+    *reinterpret_cast<float4*>(P.c[6] + base + k0) = make_float4(p7[0], p7[1], p7[2], p7[3]);
   }
 }
 
@@ -137,6 +187,76 @@ __device__ __forceinline__ float gather(const float* s, int nn, int mm, float am
   return d + dyp * (dxp * p[TN + 1] + ac);
 }
 
+// One particle of PPGRDCJPPOST2L_QP: the half push and the 8 deposited
+// quantities (cu x/y/z, dcu x/y, amu xx/yy/xy) and 4 corner weights.
+struct AmjOut {
+  float v[8];
+  float w[4];
+  float p6;
+};
+
+__device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, float dxp,
+                                          float dyp, float vx, float vy, float p6, float p7,
+                                          float qm, float qbm, float qtmh, float dti, float dex,
+                                          float idex, AmjOut* o) {
+  float amx = 1.f - dxp;
+  const float amy = 1.f - dyp;
+  const float inv_part_7 = 1.f / p7;
+  const float qtmh1 = qtmh * inv_part_7;
+  const float qtmh2 = qtmh1 * p6;
+  float dx = gather(sf[0], nn, mm, amx, amy, dxp, dyp);
+  float dy = gather(sf[1], nn, mm, amx, amy, dxp, dyp);
+  float dz = gather(sf[5], nn, mm, amx, amy, dxp, dyp);
+  float ox = gather(sf[2], nn, mm, amx, amy, dxp, dyp);
+  float oy = gather(sf[3], nn, mm, amx, amy, dxp, dyp);
+  float oz = gather(sf[4], nn, mm, amx, amy, dxp, dyp);
+  const float ddx = -1.f * qtmh2 * dx + qtmh * oy;
+  const float ddy = -1.f * qtmh2 * dy - qtmh * ox;
+  const float acx = vx + ddx, acy = vy + ddy;
+  const float omzt = qtmh1 * oz;
+  const float omt = omzt * omzt;
+  const float anorm = 2.f / (1.f + omt);
+  const float rot1 = 0.5f * (1.f - omt);
+  const float rot2 = omzt;
+  float v1 = (rot1 * acx + rot2 * acy) * anorm + ddx;
+  float v2 = (rot1 * acy - rot2 * acx) * anorm + ddy;
+  const float qm1 = qm * inv_part_7;
+  amx = qm1 * amx;
+  dxp = qm1 * dxp;
+  ox = 0.5f * (v1 + vx);
+  oy = 0.5f * (v2 + vy);
+  oz = 0.5f * (1.f + dex * dex * (ox * ox + oy * oy)) * inv_part_7 - 0.5f * p7;
+  o->p6 = p7 + oz;
+  oz = oz * idex;
+  vx = (v1 - vx) * dti;
+  vy = (v2 - vy) * dti;
+  dz = qbm * (dz + (dx * ox + dy * oy) * dex * dex * inv_part_7);
+  o->w[0] = amx * amy;
+  o->w[1] = dxp * amy;
+  o->w[2] = amx * dyp;
+  o->w[3] = dxp * dyp;
+  v1 = ox * ox * inv_part_7;
+  v2 = oy * oy * inv_part_7;
+  const float v3 = ox * oy * inv_part_7;
+  vx = vx + ox * dz * inv_part_7;
+  vy = vy + oy * dz * inv_part_7;
+  o->v[0] = ox;
+  o->v[1] = oy;
+  o->v[2] = oz;
+  o->v[3] = vx;
+  o->v[4] = vy;
+  o->v[5] = v1;
+  o->v[6] = v2;
+  o->v[7] = v3;
+}
+
+// Each thread takes 4 consecutive particles (float4 loads of each component)
+// and keeps the deposits of a run of particles in one cell in registers,
+// flushing them to the shared tile accumulators when the cell changes.  With
+// the particles of a tile stored cell by cell, this cuts the shared-memory
+// atomics about 4x and spreads a warp's atomics over different cells.
+// The per-particle products are those of the reference; only the order in
+// which a node's contributions are summed differs.
 __global__ void __launch_bounds__(256) k_amjdp(PartBuf P, TileGeom tg, GatherPlanes f,
                                                float* cux, float* cuy, float* cuz, float* dcx,
                                                float* dcy, float* amxx, float* amyy,
@@ -161,70 +281,71 @@ __global__ void __launch_bounds__(256) k_amjdp(PartBuf P, TileGeom tg, GatherPla
   const float idex = 1.f / dex;
   const int n = P.count[t];
   const long long base = (long long)t * P.cap;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const float x = P.c[0][base + k], y = P.c[1][base + k];
-    const float p6 = P.c[5][base + k], p7 = P.c[6][base + k], qm = P.c[7][base + k];
-    int nn = (int)x, mm = (int)y;
-    float dxp = x - (float)nn, dyp = y - (float)mm;
-    nn -= noffp;
-    mm -= moffp;
-    if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
-      raise_error(st, -3);
-      continue;
-    }
-    float amx = 1.f - dxp;
-    const float amy = 1.f - dyp;
-    const float inv_part_7 = 1.f / p7;
-    const float qtmh1 = qtmh * inv_part_7;
-    const float qtmh2 = qtmh1 * p6;
-    float dx = gather(sf[0], nn, mm, amx, amy, dxp, dyp);
-    float dy = gather(sf[1], nn, mm, amx, amy, dxp, dyp);
-    float dz = gather(sf[5], nn, mm, amx, amy, dxp, dyp);
-    float ox = gather(sf[2], nn, mm, amx, amy, dxp, dyp);
-    float oy = gather(sf[3], nn, mm, amx, amy, dxp, dyp);
-    float oz = gather(sf[4], nn, mm, amx, amy, dxp, dyp);
-    const float ddx = -1.f * qtmh2 * dx + qtmh * oy;
-    const float ddy = -1.f * qtmh2 * dy - qtmh * ox;
-    float vx = P.c[2][base + k], vy = P.c[3][base + k];
-    const float acx = vx + ddx, acy = vy + ddy;
-    const float omzt = qtmh1 * oz;
-    const float omt = omzt * omzt;
-    const float anorm = 2.f / (1.f + omt);
-    const float rot1 = 0.5f * (1.f - omt);
-    const float rot2 = omzt;
-    float v1 = (rot1 * acx + rot2 * acy) * anorm + ddx;
-    float v2 = (rot1 * acy - rot2 * acx) * anorm + ddy;
-    const float qm1 = qm * inv_part_7;
-    amx = qm1 * amx;
-    dxp = qm1 * dxp;
-    ox = 0.5f * (v1 + vx);
-    oy = 0.5f * (v2 + vy);
-    oz = 0.5f * (1.f + dex * dex * (ox * ox + oy * oy)) * inv_part_7 - 0.5f * p7;
-    P.c[5][base + k] = p7 + oz;
-    oz = oz * idex;
-    vx = (v1 - vx) * dti;
-    vy = (v2 - vy) * dti;
-    dz = qbm * (dz + (dx * ox + dy * oy) * dex * dex * inv_part_7);
-    const float w00 = amx * amy, w10 = dxp * amy, w01 = amx * dyp, w11 = dxp * dyp;
-    v1 = ox * ox * inv_part_7;
-    v2 = oy * oy * inv_part_7;
-    const float v3 = ox * oy * inv_part_7;
-    vx = vx + ox * dz * inv_part_7;
-    vy = vy + oy * dz * inv_part_7;
-    const int o = mm * TN + nn;
-    const int off[4] = {o, o + 1, o + TN, o + TN + 1};
-    const float w[4] = {w00, w10, w01, w11};
+  for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
+    const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
+    const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + base + k0);
+    const float4 VX = *reinterpret_cast<const float4*>(P.c[2] + base + k0);
+    const float4 VY = *reinterpret_cast<const float4*>(P.c[3] + base + k0);
+    float4 P6 = *reinterpret_cast<const float4*>(P.c[5] + base + k0);
+    const float4 P7 = *reinterpret_cast<const float4*>(P.c[6] + base + k0);
+    const float4 QM = *reinterpret_cast<const float4*>(P.c[7] + base + k0);
+    const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
+    const float vxs[4] = {VX.x, VX.y, VX.z, VX.w}, vys[4] = {VY.x, VY.y, VY.z, VY.w};
+    const float p6s[4] = {P6.x, P6.y, P6.z, P6.w}, p7s[4] = {P7.x, P7.y, P7.z, P7.w};
+    const float qms[4] = {QM.x, QM.y, QM.z, QM.w};
+    float p6o[4] = {P6.x, P6.y, P6.z, P6.w};
+    float acc[8][4];
+    int cell = -1;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      atomicAdd(&sa[0][off[c]], ox * w[c]);
-      atomicAdd(&sa[1][off[c]], oy * w[c]);
-      atomicAdd(&sa[2][off[c]], oz * w[c]);
-      atomicAdd(&sa[3][off[c]], vx * w[c]);
-      atomicAdd(&sa[4][off[c]], vy * w[c]);
-      atomicAdd(&sa[5][off[c]], v1 * w[c]);
-      atomicAdd(&sa[6][off[c]], v2 * w[c]);
-      atomicAdd(&sa[7][off[c]], v3 * w[c]);
+    for (int j = 0; j < 4; ++j) {
+      if (k0 + j < n) {
+        int nn = (int)xs[j], mm = (int)ys[j];
+        const float dxp = xs[j] - (float)nn, dyp = ys[j] - (float)mm;
+        nn -= noffp;
+        mm -= moffp;
+        if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
+          raise_error(st, -3);
+          continue;
+        }
+        AmjOut o;
+        amjdp_one(sf, nn, mm, dxp, dyp, vxs[j], vys[j], p6s[j], p7s[j], qms[j], qbm, qtmh, dti,
+                  dex, idex, &o);
+        p6o[j] = o.p6;
+        const int c = mm * TN + nn;
+        if (c != cell) {
+          if (cell >= 0) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              atomicAdd(&sa[q][cell], acc[q][0]);
+              atomicAdd(&sa[q][cell + 1], acc[q][1]);
+              atomicAdd(&sa[q][cell + TN], acc[q][2]);
+              atomicAdd(&sa[q][cell + TN + 1], acc[q][3]);
+            }
+          }
+          cell = c;
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[q][r] = o.v[q] * o.w[r];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[q][r] += o.v[q] * o.w[r];
+        }
+      }
     }
+    if (cell >= 0) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        atomicAdd(&sa[q][cell], acc[q][0]);
+        atomicAdd(&sa[q][cell + 1], acc[q][1]);
+        atomicAdd(&sa[q][cell + TN], acc[q][2]);
+        atomicAdd(&sa[q][cell + TN + 1], acc[q][3]);
+      }
+    }
+    P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
+    *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
   }
   __syncthreads();
   flush(sa[0], cux, tg, noffp, moffp, scale);

@@ -1,0 +1,222 @@
+// qp_slice.cu -- fused Fourier-space column kernels of the slice loop.
+//
+// After the x pass, column kx of every transformed component is contiguous
+// ([kx][y]).  One CTA owns one column: its warps transform the column's lines
+// along y (one warp per line), all threads then apply the Fourier-space
+// solves of the slice mode by mode, and the warps transform the results back
+// along y for the inverse x pass.  This fuses the reference's chain of
+// fftrk / pot / grad / div / elf / bf / bfqp / mult / add / fftkr calls of one
+// slice phase (simulation_class.f03:655-709, 717-726) into one launch per phase,
+// with the per-mode arithmetic of qp_solve.cuh (bit-identical to the reference).
+//
+// Kernel A, slice start (simulation_class.f03:655-675 and the first 677-680):
+//   qe, qb -> forward y; epwb = elf(qb); psi = pot(qe); fxy = grad(psi);
+//   psit = -dex * pot(div(cu)); bxyz = bf(cu); bxyz <- assembly(epw, epwb);
+//   inverse y of psi, fxy, psit, bxyz.
+// Kernel B, one predictor-corrector pass (683-709 with the next 677-680, and
+// the current extrapolation 725-726 applied to the stored cu):
+//   cu, dcu, amu -> forward y; epw = bfqp(cu, dcu, amu, epw); cu_k <- cu - dxi*dcu
+//   (x, y components); psit = -dex * pot(div(cu)); bxyz = bf(cu) + assembly;
+//   inverse y of psit, bxyz; optionally the species2d%cbq smoothing of one
+//   more line (q + cu_z) and the zeroing of the real-space accumulators.
+#include "qp_line.cuh"
+#include "qp_slice.cuh"
+#include "qp_solve.cuh"
+
+namespace qp {
+
+namespace {
+
+__device__ __forceinline__ void load_col(float* L, const float* col, int n, int lane) {
+  for (int j = lane; j <= n; j += 32) L[j] = col[j];
+  __syncwarp();
+}
+
+__device__ __forceinline__ void store_col(float* col, const float* L, int n, int lane,
+                                          float sc) {
+  for (int j = lane; j <= n; j += 32) col[j] = L[j] * sc;
+}
+
+__global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, LineTables ty,
+                                                 const DevStatus* st) {
+  extern __shared__ float smem[];
+  if (st->error) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = g.ny, npad = n + 6;
+  const int kx = blockIdx.x;
+  const long long co = (long long)kx * g.kp;
+  float* line[8];
+#pragma unroll
+  for (int w = 0; w < 8; ++w) line[w] = smem + 2 * w * npad;
+  float* L = line[warp];
+  float* S = L + npad;
+  // phase 1: forward y of qe (warp 0) and qb (warp 1)
+  if (warp == 0) {
+    load_col(L, a.qe + co, n, lane);
+    warp_line_transform(L, S, g.indy, 0, ty, lane);
+    for (int j = lane; j <= n; j += 32) L[j] *= a.norm;
+  } else if (warp == 1) {
+    if (a.qb) {
+      load_col(L, a.qb + co, n, lane);
+      warp_line_transform(L, S, g.indy, 0, ty, lane);
+      for (int j = lane; j <= n; j += 32) L[j] *= a.norm;
+    } else {
+      for (int j = lane; j <= n; j += 32) L[j] = 0.f;
+    }
+  }
+  __syncthreads();
+  // phase 2: the solves of the slice start, mode by mode
+  for (int ky = threadIdx.x; ky <= n; ky += blockDim.x) {
+    const long long o = co + ky;
+    const float q = line[0][ky], qb = line[1][ky];
+    float ebx, eby;
+    k_elf(K, kx, ky, qb, &ebx, &eby);
+    a.epwb_x[o] = ebx;
+    a.epwb_y[o] = eby;
+    const float psi = k_pot(K, kx, ky, q);
+    float fx, fy;
+    k_grad(K, kx, ky, psi, &fx, &fy);
+    const float cx = a.cu_x[o], cy = a.cu_y[o], cz = a.cu_z[o];
+    const float psit = QM(k_pot(K, kx, ky, k_div(K, kx, ky, cx, cy)), -a.dex);
+    float bx, by, bz;
+    k_bf(K, kx, ky, cx, cy, cz, &bx, &by, &bz);
+    k_assemble_mode(a.epw_x[o], a.epw_y[o], ebx, eby, a.dex, &bx, &by, &bz);
+    line[0][ky] = bz;
+    line[2][ky] = psi;
+    line[3][ky] = fx;
+    line[4][ky] = fy;
+    line[5][ky] = psit;
+    line[6][ky] = bx;
+    line[7][ky] = by;
+  }
+  __syncthreads();
+  // phase 3: inverse y; y parities: psi S, fx S, fy C, psit S, bx C, by S, bz C
+  if (warp != 1) {
+    float* dst;
+    int par;
+    switch (warp) {
+      case 0: dst = a.out_bz; par = 1; break;
+      case 2: dst = a.out_psi; par = 0; break;
+      case 3: dst = a.out_fx; par = 0; break;
+      case 4: dst = a.out_fy; par = 1; break;
+      case 5: dst = a.out_psit; par = 0; break;
+      case 6: dst = a.out_bx; par = 1; break;
+      default: dst = a.out_by; par = 0; break;
+    }
+    __syncwarp();
+    warp_line_transform(L, S, g.indy, par, ty, lane);
+    store_col(dst + co, L, n, lane, 1.f);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_slice_b(SliceB b, GridDims g, KCoef K, LineTables ty,
+                                                 DevStatus* st) {
+  extern __shared__ float smem[];
+  if (st->error) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = g.ny, npad = n + 6;
+  const int kx = blockIdx.x;
+  const long long co = (long long)kx * g.kp;
+  float* line[9];
+#pragma unroll
+  for (int w = 0; w < 8; ++w) line[w] = smem + 2 * w * npad;
+  line[8] = smem + 16 * npad;
+  float* L = line[warp];
+  float* S = L + npad;
+  // phase 1: forward y of cu(3), dcu(2), amu(3): y parities S C S, S C, S S C
+  {
+    const int par = (warp == 1 || warp == 4 || warp == 7) ? 1 : 0;
+    load_col(L, b.in[warp] + co, n, lane);
+    warp_line_transform(L, S, g.indy, par, ty, lane);
+    for (int j = lane; j <= n; j += 32) L[j] *= b.norm;
+    if (warp == 0 && b.q_in) {
+      __syncwarp();
+      float* Lq = line[8];
+      load_col(Lq, b.q_in + co, n, lane);
+      warp_line_transform(Lq, S, g.indy, 0, ty, lane);
+      for (int j = lane; j <= n; j += 32) Lq[j] *= b.norm;
+    }
+  }
+  __syncthreads();
+  // phase 2: corrector, extrapolated current, psit and bxyz of the next pass
+  float r_num = 0.f, r_den = 0.f;
+  for (int ky = threadIdx.x; ky <= n; ky += blockDim.x) {
+    const long long o = co + ky;
+    const float cx = line[0][ky], cy = line[1][ky], cz = line[2][ky];
+    float dcx = line[3][ky], dcy = line[4][ky];
+    const float axx = line[5][ky], ayy = line[6][ky], axy = line[7][ky];
+    const float ex0 = b.epw_x[o], ey0 = b.epw_y[o];
+    float ex = ex0, ey = ey0;
+    k_bfqp(K, kx, ky, b.aa, b.idex, cz, &dcx, &dcy, axx, ayy, axy, &ex, &ey);
+    b.epw_x[o] = ex;
+    b.epw_y[o] = ey;
+    r_num += (ex - ex0) * (ex - ex0) + (ey - ey0) * (ey - ey0);
+    r_den += ex * ex + ey * ey;
+    // dcu = dcu * dxi; cu(1:2) = cu(1:2) - dcu(1:2)  (kept for the next slice)
+    b.cu_x[o] = QS(cx, QM(dcx, b.dxi));
+    b.cu_y[o] = QS(cy, QM(dcy, b.dxi));
+    b.cu_z[o] = cz;
+    const float psit = QM(k_pot(K, kx, ky, k_div(K, kx, ky, cx, cy)), -b.dex);
+    float bx, by, bz;
+    k_bf(K, kx, ky, cx, cy, cz, &bx, &by, &bz);
+    k_assemble_mode(ex, ey, b.epwb_x[o], b.epwb_y[o], b.dex, &bx, &by, &bz);
+    line[0][ky] = psit;
+    line[1][ky] = bx;
+    line[2][ky] = by;
+    line[3][ky] = bz;
+    if (b.q_in) line[8][ky] = k_smooth(K, kx, ky, line[8][ky]);
+  }
+  // relative change of B_perp for the convergence-controlled iteration
+  r_num = warp_sum(r_num);
+  r_den = warp_sum(r_den);
+  if (lane == 0 && b.track_residual) {
+    atomicAdd(&st->resid_num, r_num);
+    atomicAdd(&st->resid_den, r_den);
+  }
+  __syncthreads();
+  // phase 3: inverse y of psit (S), bx (C), by (S), bz (C) and the smoothed q (S)
+  if (warp < 4) {
+    const int par = (warp == 1 || warp == 3) ? 1 : 0;
+    warp_line_transform(L, S, g.indy, par, ty, lane);
+    store_col(b.out[warp] + co, L, n, lane, 1.f);
+  } else if (warp == 4 && b.q_in) {
+    float* Lq = line[8];
+    warp_line_transform(Lq, S, g.indy, 0, ty, lane);
+    store_col(b.q_out + co, Lq, n, lane, 1.f);
+  } else if (warp >= 5 && b.nzero) {
+    // zero the real-space accumulators for the next pass (their values were
+    // consumed by the x pass that precedes this kernel)
+    const long long per = (g.rplane + gridDim.x - 1) / gridDim.x;
+    const long long lo = per * kx, hi = min(g.rplane, lo + per);
+    for (int z = 0; z < b.nzero; ++z)
+      for (long long i = lo + (threadIdx.x - 160); i < hi; i += 96) b.zero[z][i] = 0.f;
+  }
+}
+
+}  // namespace
+
+size_t slice_a_smem(const GridDims& g) { return sizeof(float) * 16 * (size_t)(g.ny + 6); }
+size_t slice_b_smem(const GridDims& g) { return sizeof(float) * 17 * (size_t)(g.ny + 6); }
+
+int slice_kernels_init() {
+  const int big = (int)(sizeof(float) * 17 * ((1 << QP_MAX_IND) + 6));
+  if (cudaFuncSetAttribute(k_slice_a, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+      cudaSuccess)
+    return -2;
+  if (cudaFuncSetAttribute(k_slice_b, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+      cudaSuccess)
+    return -2;
+  return 0;
+}
+
+void launch_slice_a(const SliceA& a, const GridDims& g, const KCoef& K, const LineTables& ty,
+                    const DevStatus* st, cudaStream_t s) {
+  k_slice_a<<<g.nx + 1, 256, slice_a_smem(g), s>>>(a, g, K, ty, st);
+}
+
+void launch_slice_b(const SliceB& b, const GridDims& g, const KCoef& K, const LineTables& ty,
+                    DevStatus* st, cudaStream_t s) {
+  k_slice_b<<<g.nx + 1, 256, slice_b_smem(g), s>>>(b, g, K, ty, st);
+}
+
+}  // namespace qp

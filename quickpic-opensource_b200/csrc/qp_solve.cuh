@@ -13,11 +13,18 @@
 //   grad   MPPGRADFD2     fft2d_lib77.f:9231-9295
 // ffre/ffim are the real and imaginary parts of the form-factor table ffd
 // (affp*s/k^2, s), stored [kx][ky] with pitch ny, kx < nx, ky < ny.
+// All arithmetic uses round-to-nearest intrinsics in the reference's
+// left-to-right order, so no multiply-add is contracted and each mode is
+// bit-identical to the reference's FP32 build whatever the compile flags.
 #pragma once
 
 #include "qp_common.cuh"
 
 namespace qp {
+
+#define QM(a, b) __fmul_rn((a), (b))
+#define QA(a, b) __fadd_rn((a), (b))
+#define QS(a, b) __fsub_rn((a), (b))
 
 struct KCoef {
   int nx, ny;
@@ -32,20 +39,20 @@ struct KCoef {
 };
 
 __device__ __forceinline__ float k_pot(const KCoef& K, int kx, int ky, float q) {
-  return K.interior(kx, ky) ? K.re(kx, ky) * q : 0.f;
+  return K.interior(kx, ky) ? QM(K.re(kx, ky), q) : 0.f;
 }
 
 __device__ __forceinline__ float k_smooth(const KCoef& K, int kx, int ky, float q) {
-  return K.interior(kx, ky) ? K.im(kx, ky) * q : 0.f;
+  return K.interior(kx, ky) ? QM(K.im(kx, ky), q) : 0.f;
 }
 
 __device__ __forceinline__ void k_elf(const KCoef& K, int kx, int ky, float q, float* fx,
                                       float* fy) {
   if (K.interior(kx, ky)) {
-    const float at1 = K.re(kx, ky) * K.im(kx, ky);
-    const float at3 = -at1 * q;
-    *fx = (K.dnx * (float)kx) * at3;
-    *fy = (K.dny * (float)ky) * at3;
+    const float at1 = QM(K.re(kx, ky), K.im(kx, ky));
+    const float at3 = QM(-at1, q);
+    *fx = QM(QM(K.dnx, (float)kx), at3);
+    *fy = QM(QM(K.dny, (float)ky), at3);
   } else {
     *fx = 0.f;
     *fy = 0.f;
@@ -58,21 +65,21 @@ __device__ __forceinline__ void k_bf(const KCoef& K, int kx, int ky, float cux, 
   *by = 0.f;
   *bz = 0.f;
   if (kx >= K.nx || ky >= K.ny) return;
-  const float dkx = K.dnx * (float)kx;
-  const float dky = K.dny * (float)ky;
+  const float dkx = QM(K.dnx, (float)kx);
+  const float dky = QM(K.dny, (float)ky);
   if (kx > 0) {
-    const float at1 = K.re(kx, ky) * K.im(kx, ky);
+    const float at1 = QM(K.re(kx, ky), K.im(kx, ky));
     if (ky > 0) {
-      const float at2 = dky * at1, at3 = dkx * at1;
-      *bx = at2 * cuz;
-      *by = -at3 * cuz;
-      *bz = at3 * cuy - at2 * cux;
+      const float at2 = QM(dky, at1), at3 = QM(dkx, at1);
+      *bx = QM(at2, cuz);
+      *by = QM(-at3, cuz);
+      *bz = QS(QM(at3, cuy), QM(at2, cux));
     } else {
-      *bz = (dkx * at1) * cuy;
+      *bz = QM(QM(dkx, at1), cuy);
     }
   } else if (ky > 0) {
-    const float at1 = K.re(0, ky) * K.im(0, ky);
-    *bz = -(dky * at1) * cux;
+    const float at1 = QM(K.re(0, ky), K.im(0, ky));
+    *bz = QM(-QM(dky, at1), cux);
   }
 }
 
@@ -85,38 +92,38 @@ __device__ __forceinline__ void k_bfqp(const KCoef& K, int kx, int ky, float aa,
   *bx = 0.f;
   *by = 0.f;
   if (kx >= K.nx || ky >= K.ny) return;
-  const float dkx = K.dnx * (float)kx;
-  const float dky = K.dny * (float)ky;
+  const float dkx = QM(K.dnx, (float)kx);
+  const float dky = QM(K.dny, (float)ky);
   if (kx > 0) {
     if (ky > 0) {
-      const float d1 = -*dcx + dkx * amxx - dky * amxy;
-      const float aat1 = d1 - dkx * cuz * idex;
-      const float d2 = -*dcy - dkx * amxy + dky * amyy;
-      const float aat2 = d2 - dky * cuz * idex;
+      const float d1 = QS(QA(-*dcx, QM(dkx, amxx)), QM(dky, amxy));
+      const float aat1 = QS(d1, QM(QM(dkx, cuz), idex));
+      const float d2 = QA(QS(-*dcy, QM(dkx, amxy)), QM(dky, amyy));
+      const float aat2 = QS(d2, QM(QM(dky, cuz), idex));
       float at2 = K.re(kx, ky);
-      at2 = at2 / (1.f + aa * at2);
-      const float at1 = at2 * K.im(kx, ky);
-      *bx = at1 * aat1 + aa * at2 * bxo;
-      *by = at1 * aat2 + aa * at2 * byo;
+      at2 = __fdiv_rn(at2, QA(1.f, QM(aa, at2)));
+      const float at1 = QM(at2, K.im(kx, ky));
+      *bx = QA(QM(at1, aat1), QM(QM(aa, at2), bxo));
+      *by = QA(QM(at1, aat2), QM(QM(aa, at2), byo));
       *dcx = d1;
       *dcy = d2;
     } else {
-      const float d1 = -*dcx + dkx * amxx;
-      const float d2 = -*dcy - dkx * amxy;
+      const float d1 = QA(-*dcx, QM(dkx, amxx));
+      const float d2 = QS(-*dcy, QM(dkx, amxy));
       float at2 = K.re(kx, 0);
-      at2 = at2 / (1.f + aa * at2);
-      const float at1 = at2 * K.im(kx, 0);
-      *by = at1 * d2 + aa * at2 * byo;
+      at2 = __fdiv_rn(at2, QA(1.f, QM(aa, at2)));
+      const float at1 = QM(at2, K.im(kx, 0));
+      *by = QA(QM(at1, d2), QM(QM(aa, at2), byo));
       *dcx = d1;
       *dcy = d2;
     }
   } else if (ky > 0) {
-    const float d1 = -*dcx - dky * amxy;
-    const float d2 = -*dcy + dky * amyy;
+    const float d1 = QS(-*dcx, QM(dky, amxy));
+    const float d2 = QA(-*dcy, QM(dky, amyy));
     float at2 = K.re(0, ky);
-    at2 = at2 / (1.f + aa * at2);
-    const float at1 = at2 * K.im(0, ky);
-    *bx = at1 * d1 + aa * at2 * bxo;
+    at2 = __fdiv_rn(at2, QA(1.f, QM(aa, at2)));
+    const float at1 = QM(at2, K.im(0, ky));
+    *bx = QA(QM(at1, d1), QM(QM(aa, at2), bxo));
     *dcx = d1;
     *dcy = d2;
   }
@@ -124,18 +131,27 @@ __device__ __forceinline__ void k_bfqp(const KCoef& K, int kx, int ky, float aa,
 
 __device__ __forceinline__ float k_div(const KCoef& K, int kx, int ky, float fx, float fy) {
   if (!K.interior(kx, ky)) return 0.f;
-  return -((K.dnx * (float)kx) * fx + (K.dny * (float)ky) * fy);
+  return -QA(QM(QM(K.dnx, (float)kx), fx), QM(QM(K.dny, (float)ky), fy));
 }
 
 __device__ __forceinline__ void k_grad(const KCoef& K, int kx, int ky, float p, float* fx,
                                        float* fy) {
   if (K.interior(kx, ky)) {
-    *fx = (K.dnx * (float)kx) * p;
-    *fy = (K.dny * (float)ky) * p;
+    *fx = QM(QM(K.dnx, (float)kx), p);
+    *fy = QM(QM(K.dny, (float)ky), p);
   } else {
     *fx = 0.f;
     *fy = 0.f;
   }
+}
+
+// bxyz assembly of one mode (simulation_class.f03:677-680 and 717-720):
+//   bx = epw(2)*(-dex) - epwb(2); by = epw(1)*dex + epwb(1); bz = bz*dex
+__device__ __forceinline__ void k_assemble_mode(float ex, float ey, float ebx, float eby,
+                                                float dex, float* bx, float* by, float* bz) {
+  *bx = QS(QM(ey, -dex), eby);
+  *by = QA(QM(ex, dex), ebx);
+  *bz = QM(*bz, dex);
 }
 
 // standalone launches used by the class-level API
