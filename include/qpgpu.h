@@ -237,6 +237,11 @@ int qp_sim_download_field(qp_sim* sim, const char* name, float* out);
 /* 3D fields (3, nx+2, ny+1, nz+1): "bexyz" or "bbxyz"; species 3D charge
  * (nx+2, ny+1, nz+1): "q3". */
 int qp_sim_download_3d(qp_sim* sim, const char* name, float* out);
+/* Component comp (1..3) of the 3D field bexyz on the axis node (nx/2, ny/2)
+ * of every slice: out(nz+1), the on-axis wake lineout.  A 1D cut of the 3D
+ * field that the reference's field slice diagnostics write to HDF5 files
+ * (init_diag, simulation_class.f03:771-1100), read here without a file. */
+int qp_sim_download_lineout(qp_sim* sim, int comp, float* out);
 /* Per-kernel device times of the first `nslices` slices of a 3D step, run
  * without graphs with an event pair around every launch (the timing side of
  * the reference's per-step ELOG stamps, simulation_class.f03:614-645).
