@@ -155,6 +155,33 @@ int qp_species_push(qp_species* sp, qp_field2d* fxy, qp_field2d* bxyz, qp_field2
 int qp_species_partpush(qp_species* sp, qp_field2d* fxy, qp_field2d* bxyz, qp_field2d* psit,
                         float dex);
 int qp_species_pmove(qp_species* sp);
+/* The re-bin of qp_species_pmove for callers that cannot allocate device
+ * memory while they run (a host code whose allocator owns the GPU's memory,
+ * or a job held to a fixed memory budget).  This entry point has no
+ * counterpart in the reference.  The caller owns both particle buffers, as
+ * device pointers: part_in[8] / part_out[8] hold the eight component planes
+ * of ntiles * cap floats (tile t in [t*cap, t*cap + count[t])), count_in /
+ * count_out one int per tile; ntiles = (2^indx / 16) * (2^indy / 16).  The
+ * output equals qp_species_pmove's on the same input.  The mover inbox and
+ * the status live in one fixed device array of
+ * QP_PMOVE_STATIC_SCRATCH_BYTES, which every GPU that loads the library holds
+ * until the process exits; no call allocates or frees device memory.  The
+ * inbox takes min(16384, about 16 MiB / (40 B * ntiles)) movers per tile
+ * (408 on a 512 x 512 grid, 100 on 1024 x 1024); grids that leave fewer than
+ * QP_PMOVE_STATIC_MIN_INBOX are rejected, and so is a step that moves more
+ * particles into one tile, or fills an output tile beyond cap_out: those
+ * return -1 with the sizes in qp_ctx_last_error(NULL) and leave the input
+ * untouched (there is no grow-and-retry).  The first call on each device
+ * looks up the array's device address, so make that call before any stream
+ * capture.  Every call shares the one array: calls that overlap on the GPU
+ * (other streams, other host threads) race.  The call runs on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and returns after it
+ * has synchronised that stream. */
+#define QP_PMOVE_STATIC_SCRATCH_BYTES (16u << 20)
+#define QP_PMOVE_STATIC_MIN_INBOX 64
+int qp_pmove_static(int indx, int indy, const float* const* part_in, const int* count_in,
+                    int cap_in, float* const* part_out, int* count_out, int cap_out,
+                    void* stream);
 /* species2d%cbq (399-418): q_species(1) += cu_species(3); smooth; store as
  * slice `pos` (1-based) of the species' 3D charge q3. */
 int qp_species_cbq(qp_species* sp, int pos);
