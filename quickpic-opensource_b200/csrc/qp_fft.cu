@@ -56,16 +56,23 @@ void line_tables_free(LineTablesHost* t) {
 }
 
 // ------------------------------------------------------------------ x pass
+// Shared memory of the line kernels: 8 lines of pitch n + 4 floats (16-byte
+// aligned rows; the transposed accesses below hit 32 distinct banks), plus 8
+// scratch lines for lines shorter than 64 points.
+static __host__ __device__ int line_pitch(int n) { return n + 4; }
+static __host__ __device__ int line_count(int logn) { return logn < 6 ? 16 : 8; }
+
 // Forward x pass: for every component c and row y, the line
 //   x[j] = scale_c * (src_c[y][j] + src2_c[y][j]),  j = 0..nx
 // is transformed with parity_c and stored transposed into dst_c[kx][y].
+template <int P>
 __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables tx,
                                               const DevStatus* st) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = g.nx, npad = n + 6;
-  float* L = smem + (2 * warp) * npad;
-  float* S = L + npad;
+  const int n = g.nx, pitch = line_pitch(n);
+  float* L = smem + warp * pitch;
+  float* S = smem + (8 + warp) * pitch;
   if (st && st->error) return;
   const XComp c = job.c[blockIdx.y];
   const int y0 = blockIdx.x * 8;
@@ -75,51 +82,46 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
   if (y <= g.ny) {
     const float* s1 = c.src + cur + (long long)y * g.rp;
     const float* s2 = c.src2 ? c.src2 + (long long)y * g.rp : nullptr;
-    for (int j = lane; j <= n; j += 32) {
-      float v = s1[j];
-      if (s2) v += s2[j];
-      L[j] = v * c.scale;
-    }
-    __syncwarp();
-    warp_line_transform(L, S, g.indx, c.parity, tx, lane);
+    line_transform<P>(s1, s2, c.scale, L, S, g.indx, c.parity, tx, lane);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
     const int r = idx & 7, kx = idx >> 3;
     const int yy = y0 + r;
-    if (yy <= g.ny) c.dst[(long long)kx * g.kp + yy] = smem[(2 * r) * npad + kx];
+    if (yy <= g.ny) c.dst[(long long)kx * g.kp + yy] = smem[r * pitch + kx];
   }
 }
 
 // Inverse x pass: rows y of the [kx][y] array are gathered, transformed with
 // parity_c, scaled and written as real-space rows; row 0 is also written to the
 // guard row ny (copyguard), and the line computed for row ny is discarded.
+template <int P>
 __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables tx,
                                               const DevStatus* st) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = g.nx, npad = n + 6;
+  const int n = g.nx, pitch = line_pitch(n);
   if (st && st->error) return;
   const XComp c = job.c[blockIdx.y];
   const int y0 = blockIdx.x * 8;
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
     const int r = idx & 7, kx = idx >> 3;
     const int yy = y0 + r;
-    smem[(2 * r) * npad + kx] = (yy <= g.ny) ? c.src[(long long)kx * g.kp + yy] : 0.f;
+    smem[r * pitch + kx] = (yy <= g.ny) ? c.src[(long long)kx * g.kp + yy] : 0.f;
   }
   __syncthreads();
-  float* L = smem + (2 * warp) * npad;
-  float* S = L + npad;
+  float* L = smem + warp * pitch;
+  float* S = smem + (8 + warp) * pitch;
   const int y = y0 + warp;
   if (y < g.ny) {
-    warp_line_transform(L, S, g.indx, c.parity, tx, lane);
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indx, c.parity, tx, lane);
     long long cur = 0;
     if (c.cursor_stride) cur = (long long)st->cursor * c.cursor_stride;
     float* d = c.dst + cur + (long long)y * g.rp;
-    for (int j = lane; j <= n; j += 32) d[j] = L[j] * c.scale;
+    line_store(d, L, n, c.scale, lane);
     if (y == 0) {
       float* dg = c.dst + cur + (long long)g.ny * g.rp;
-      for (int j = lane; j <= n; j += 32) dg[j] = L[j] * c.scale;
+      line_store(dg, L, n, c.scale, lane);
       if (lane == 0) dg[n + 1] = d[n + 1];
     }
   }
@@ -132,60 +134,70 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
 
 // ------------------------------------------------------------------ y pass
 // In-place y transform of the columns kx of every component, times scale_c.
+template <int P>
 __global__ void __launch_bounds__(256) k_ycol(YJob job, GridDims g, LineTables ty,
                                               const DevStatus* st) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   if (st && st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = g.ny, npad = n + 6;
-  float* L = smem + (2 * warp) * npad;
-  float* S = L + npad;
+  const int n = g.ny, pitch = line_pitch(n);
+  float* L = smem + warp * pitch;
+  float* S = smem + (8 + warp) * pitch;
   const int kx = blockIdx.x * 8 + warp;
   if (kx > g.nx) return;
   for (int ci = 0; ci < job.ncomp; ++ci) {
     float* col = job.c[ci].plane + (long long)kx * g.kp;
-    for (int j = lane; j <= n; j += 32) L[j] = col[j];
-    __syncwarp();
-    warp_line_transform(L, S, g.indy, job.c[ci].parity, ty, lane);
-    const float sc = job.c[ci].scale;
-    for (int j = lane; j <= n; j += 32) col[j] = L[j] * sc;
+    line_transform<P>(col, nullptr, 1.f, L, S, g.indy, job.c[ci].parity, ty, lane);
+    line_store(col, L, n, job.c[ci].scale, lane);
     __syncwarp();
   }
 }
 
-size_t xpass_smem(const GridDims& g) { return sizeof(float) * 16 * (size_t)(g.nx + 6); }
-size_t ypass_smem(const GridDims& g) { return sizeof(float) * 16 * (size_t)(g.ny + 6); }
+size_t xpass_smem(const GridDims& g) {
+  return sizeof(float) * line_count(g.indx) * (size_t)line_pitch(g.nx);
+}
+size_t ypass_smem(const GridDims& g) {
+  return sizeof(float) * line_count(g.indy) * (size_t)line_pitch(g.ny);
+}
+
+template <int P>
+static int set_smem_limits(int big) {
+  if (cudaFuncSetAttribute(k_xfwd<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_xinv<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_ycol<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+          cudaSuccess)
+    return -2;
+  return 0;
+}
 
 int fft_kernels_init() {
-  const int big = (int)(sizeof(float) * 16 * ((1 << QP_MAX_IND) + 6));
-  if (cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
-      cudaSuccess)
-    return -2;
-  if (cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
-      cudaSuccess)
-    return -2;
-  if (cudaFuncSetAttribute(k_ycol, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
-      cudaSuccess)
-    return -2;
+  const int big = (int)(sizeof(float) * 8 * line_pitch(1 << QP_MAX_IND));
+  for (int logn = 4; logn <= QP_MAX_IND; ++logn) {
+    int rc = 0;
+    QP_LINE_SWITCH(logn, rc = set_smem_limits<P_>(big));
+    if (rc) return rc;
+  }
   return 0;
 }
 
 void launch_xfwd(const XJob& job, const GridDims& g, const LineTables& tx, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.ny + 1 + 7) / 8, job.ncomp);
-  k_xfwd<<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st);
+  QP_LINE_SWITCH(g.indx, (k_xfwd<P_><<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st)));
 }
 
 void launch_xinv(const XJob& job, const GridDims& g, const LineTables& tx, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.ny + 1 + 7) / 8, job.ncomp);
-  k_xinv<<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st);
+  QP_LINE_SWITCH(g.indx, (k_xinv<P_><<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st)));
 }
 
 void launch_ycol(const YJob& job, const GridDims& g, const LineTables& ty, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.nx + 1 + 7) / 8);
-  k_ycol<<<grid, 256, ypass_smem(g), s>>>(job, g, ty, st);
+  QP_LINE_SWITCH(g.indy, (k_ycol<P_><<<grid, 256, ypass_smem(g), s>>>(job, g, ty, st)));
 }
 
 }  // namespace qp

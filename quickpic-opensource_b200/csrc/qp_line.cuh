@@ -188,4 +188,248 @@ static __device__ __noinline__ void warp_line_transform(float* L, float* S, int 
   __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident form of the same transform for n = 64 P (P = 1..32).
+//
+// The n/2-point complex FFT is split as n/2 = P * 32: lane l holds the points
+// m = l + 32 a (a = 0..P-1) in registers.  A P-point DFT over a runs in the
+// lane's registers.  After a twiddle by exp(-2 pi i l k2 / (n/2)), a 32-point
+// DFT over l runs across the lanes (radix-2 decimation in frequency with
+// shuffles), which leaves Z[k2 + P * brev5(l)] in register k2 of lane l.  The
+// pre-twiddle partners x[n - j], the unscramble partners Z[n/2 - k] and the
+// prefix sum of the odd outputs are all lane shuffles, so the only memory
+// traffic is the load of the line and one store of the result.
+
+__device__ __forceinline__ int brev5(int v) { return (int)(__brev((unsigned)v) >> 27); }
+
+template <int P>
+__host__ __device__ constexpr int brev_p(int v) {
+  int r = 0;
+  for (int b = 1, rb = P >> 1; b < P; b <<= 1, rb >>= 1)
+    if (v & b) r |= rb;
+  return r;
+}
+
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+__device__ __forceinline__ float2 shfl2(float2 v, int src) {
+  return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// Unnormalised DST-I (parity 0) / DCT-I (parity 1) of the line
+//   x[j] = in_scale * (in[j] + in2[j]),  j = 0..n   (in2 may be null)
+// written to out[0..n] (shared memory, 16-byte aligned; may alias `in`).
+// `in` and `in2` may point to global or shared memory, 8-byte aligned.
+template <int P>
+__device__ __forceinline__ void reg_line(const float* in, const float* in2, float in_scale,
+                                         float* out, int parity, const LineTables& t, int lane) {
+  constexpr int N = 64 * P;
+  const unsigned FULL = 0xffffffffu;
+  // 1. the line: x[2m], x[2m+1] for m = lane + 32 a, and x[n]
+  float2 xp[P];
+#pragma unroll
+  for (int a = 0; a < P; ++a) {
+    const int m = lane + 32 * a;
+    float2 v = *reinterpret_cast<const float2*>(in + 2 * m);
+    if (in2) {
+      const float2 w = *reinterpret_cast<const float2*>(in2 + 2 * m);
+      v.x += w.x;
+      v.y += w.y;
+    }
+    xp[a] = make_float2(v.x * in_scale, v.y * in_scale);
+  }
+  float xn = 0.f;
+  if (lane == 0) {
+    xn = in[N];
+    if (in2) xn += in2[N];
+    xn *= in_scale;
+  }
+  __syncwarp();
+  float sigma = 0.f;
+  if (parity) {
+    // sigma = 0.5 (x[0] - x[n]) + sum_{j=1}^{n-1} x[j] cos(pi j / n)
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+      const int j = 2 * (lane + 32 * a);
+      if (j) acc += xp[a].x * t.cs[j];
+      acc += xp[a].y * t.cs[j + 1];
+    }
+    acc = warp_sum(acc);
+    sigma = __shfl_sync(FULL, 0.5f * (xp[0].x - xn), 0) + acc;
+  }
+  // 2. pre-twiddle: z[a] = y[2m] + i y[2m+1]
+  float2 z[P];
+#pragma unroll
+  for (int a = 0; a < P; ++a) {
+    const int m = lane + 32 * a;
+    float r0 = __shfl_sync(FULL, xp[P - 1 - a].x, (32 - lane) & 31);  // x[n - 2m]
+    if (lane == 0) r0 = (a == 0) ? xn : xp[(P - a) % P].x;
+    const float r1 = __shfl_xor_sync(FULL, xp[P - 1 - a].y, 31);  // x[n - 2m - 1]
+    const int j0 = 2 * m, j1 = 2 * m + 1;
+    const float s0 = t.sn[min(j0, N - j0)], s1 = t.sn[min(j1, N - j1)];
+    const float x0 = xp[a].x, x1 = xp[a].y;
+    float y0, y1;
+    if (parity == 0) {
+      y0 = (m == 0) ? 0.f : s0 * (x0 + r0) + 0.5f * (x0 - r0);
+      y1 = s1 * (x1 + r1) + 0.5f * (x1 - r1);
+    } else {
+      y0 = 0.5f * (x0 + r0) - s0 * (x0 - r0);
+      y1 = 0.5f * (x1 + r1) - s1 * (x1 - r1);
+    }
+    z[a] = make_float2(y0, y1);
+  }
+  // 3. P-point DFT over a in registers (radix-2 DIF, output in bit-reversed order);
+  //    exp(-2 pi i k / 32) = tw[k P]
+#pragma unroll
+  for (int s = P / 2; s >= 1; s >>= 1) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (!(i & s)) {
+        const float2 A = z[i], B = z[i + s];
+        z[i] = make_float2(A.x + B.x, A.y + B.y);
+        float2 D = make_float2(A.x - B.x, A.y - B.y);
+        const int k = (i & (s - 1)) * (16 / s);
+        if (k) D = cmul(D, t.tw[k * P]);
+        z[i + s] = D;
+      }
+    }
+  }
+  float2 w[P];
+#pragma unroll
+  for (int k2 = 0; k2 < P; ++k2) w[k2] = z[brev_p<P>(k2)];
+  // 4. twiddle exp(-2 pi i lane k2 / (n/2))
+#pragma unroll
+  for (int k2 = 1; k2 < P; ++k2) w[k2] = cmul(w[k2], t.tw[lane * k2]);
+  // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles)
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool hi = (lane & s) != 0;
+    const float2 tws = hi ? t.tw[(lane & (s - 1)) * (16 / s) * P] : make_float2(1.f, 0.f);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+      const float2 v = w[k2];
+      const float2 p = shfl_xor2(v, s);
+      const float2 d = hi ? make_float2(p.x - v.x, p.y - v.y) : make_float2(v.x + p.x, v.y + p.y);
+      w[k2] = hi ? cmul(d, tws) : d;
+    }
+  }
+  // 6. real-FFT unscramble: Y[k] = sum_j y[j] exp(-2 pi i j k / n), k = k2 + P k1
+  const int k1 = brev5(lane);
+  const int src0 = brev5((32 - k1) & 31);
+  float ev[P], od[P];
+  float yh = 0.f;
+  float run = 0.f;
+#pragma unroll
+  for (int k2 = 0; k2 < P; ++k2) {
+    float2 B = (k2 == 0) ? shfl2(w[0], src0) : shfl_xor2(w[(P - k2) % P], 31);
+    B.y = -B.y;
+    const int k = k2 + P * k1;
+    const float2 A = w[k2];
+    float2 Y;
+    if (k == 0) {
+      Y = make_float2(A.x + A.y, 0.f);
+      yh = A.x - A.y;
+    } else {
+      const float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y + B.y));
+      const float2 D = make_float2(A.x - B.x, A.y - B.y);
+      const float2 q = cmul(t.uw[k], D);
+      Y = make_float2(E.x + 0.5f * q.y, E.y - 0.5f * q.x);
+    }
+    // sine:   out[2k] = -2 Im Y[k], out[2k+1] = Re Y[0] + 2 sum_{m=1..k} Re Y[m]
+    // cosine: out[2k] =  2 Re Y[k], out[2k+1] = 2 sigma - 2 sum_{m=1..k} Im Y[m]
+    float term;
+    if (parity == 0) {
+      ev[k2] = (k == 0) ? 0.f : -2.f * Y.y;
+      term = (k == 0) ? Y.x : 2.f * Y.x;
+    } else {
+      ev[k2] = 2.f * Y.x;
+      term = (k == 0) ? 0.f : -2.f * Y.y;
+    }
+    run += term;
+    od[k2] = run;
+  }
+  // 7. exclusive scan of the block sums in block order k1
+  const float blk = __shfl_sync(FULL, run, k1);  // lane l: sum of block l
+  float inc = blk;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float u = __shfl_up_sync(FULL, inc, o);
+    if (lane >= o) inc += u;
+  }
+  float base = __shfl_sync(FULL, inc - blk, k1);
+  if (parity) base += 2.f * sigma;
+  __syncwarp();
+  // 8. out[2k], out[2k+1] for the lane's block k = P k1 .. P k1 + P - 1
+  float* o = out + 2 * P * k1;
+  if (P == 1) {
+    *reinterpret_cast<float2*>(o) = make_float2(ev[0], base + od[0]);
+  } else {
+#pragma unroll
+    for (int k2 = 0; k2 < P; k2 += 2)
+      *reinterpret_cast<float4*>(o + 2 * k2) =
+          make_float4(ev[k2], base + od[k2], ev[(k2 + 1) % P], base + od[(k2 + 1) % P]);
+  }
+  if (lane == 0) out[N] = parity ? 2.f * yh : 0.f;
+  __syncwarp();
+}
+
+// Per-warp line transform of x = in_scale * (in + in2) into the shared line
+// `sline` (16-byte aligned, n + 4 floats).  P = n / 64 selects the register
+// form; P = 0 (lines shorter than 64 points) goes through `sline` and the
+// shared scratch `sscr` (n + 4 floats) with the shared-memory form.  Kernels
+// are instantiated per P (QP_LINE_SWITCH) so that each holds only the
+// registers its line length needs.
+template <int P>
+__device__ __forceinline__ void line_transform(const float* in, const float* in2, float in_scale,
+                                               float* sline, float* sscr, int logn, int parity,
+                                               const LineTables& t, int lane) {
+  if constexpr (P > 0) {
+    reg_line<P>(in, in2, in_scale, sline, parity, t, lane);
+  } else {
+    const int n = 1 << logn;
+    float v[2];
+    // the line may alias sline: read everything before writing
+    int c = 0;
+    for (int j = lane; j <= n; j += 32) {
+      float x = in[j];
+      if (in2) x += in2[j];
+      v[c++] = x * in_scale;
+    }
+    __syncwarp();
+    c = 0;
+    for (int j = lane; j <= n; j += 32) sline[j] = v[c++];
+    __syncwarp();
+    warp_line_transform(sline, sscr, logn, parity, t, lane);
+  }
+}
+
+constexpr int line_p(int logn) { return logn < 6 ? 0 : 1 << (logn - 6); }
+
+// Runs STMT with the compile-time constant P_ = line_p(logn).
+#define QP_LINE_SWITCH(logn, STMT)                \
+  switch (logn) {                                 \
+    case 6: { constexpr int P_ = 1; STMT; } break;   \
+    case 7: { constexpr int P_ = 2; STMT; } break;   \
+    case 8: { constexpr int P_ = 4; STMT; } break;   \
+    case 9: { constexpr int P_ = 8; STMT; } break;   \
+    case 10: { constexpr int P_ = 16; STMT; } break; \
+    case 11: { constexpr int P_ = 32; STMT; } break; \
+    default: { constexpr int P_ = 0; STMT; } break;  \
+  }
+
+// Coalesced copy of a shared line (n + 1 floats) to global memory, times sc.
+__device__ __forceinline__ void line_store(float* dst, const float* sline, int n, float sc,
+                                           int lane) {
+  const float4* s4 = reinterpret_cast<const float4*>(sline);
+  float4* d4 = reinterpret_cast<float4*>(dst);
+  for (int i = lane; i < (n >> 2); i += 32) {
+    const float4 v = s4[i];
+    d4[i] = make_float4(v.x * sc, v.y * sc, v.z * sc, v.w * sc);
+  }
+  if (lane == 0) dst[n] = sline[n] * sc;
+}
+
 }  // namespace qp

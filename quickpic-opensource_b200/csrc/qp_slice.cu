@@ -27,42 +27,32 @@ namespace qp {
 
 namespace {
 
-__device__ __forceinline__ void load_col(float* L, const float* col, int n, int lane) {
-  for (int j = lane; j <= n; j += 32) L[j] = col[j];
-  __syncwarp();
-}
+// Shared lines of pitch n + 4 floats; lines shorter than 64 points also need
+// one scratch line per warp (line_transform's shared-memory form).
+__host__ __device__ int col_pitch(int n) { return n + 4; }
 
-__device__ __forceinline__ void store_col(float* col, const float* L, int n, int lane,
-                                          float sc) {
-  for (int j = lane; j <= n; j += 32) col[j] = L[j] * sc;
-}
-
+template <int P>
 __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, LineTables ty,
                                                  const DevStatus* st) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   if (st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = g.ny, npad = n + 6;
+  const int n = g.ny, pitch = col_pitch(n);
   const int kx = blockIdx.x;
   const long long co = (long long)kx * g.kp;
   float* line[8];
 #pragma unroll
-  for (int w = 0; w < 8; ++w) line[w] = smem + 2 * w * npad;
-  float* L = line[warp];
-  float* S = L + npad;
+  for (int w = 0; w < 8; ++w) line[w] = smem + w * pitch;
+  float* L = smem + warp * pitch;
+  float* S = smem + (8 + warp) * pitch;
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
   if (warp == 0) {
-    load_col(L, a.qe + co, n, lane);
-    warp_line_transform(L, S, g.indy, 0, ty, lane);
-    for (int j = lane; j <= n; j += 32) L[j] *= a.norm;
+    line_transform<P>(a.qe + co, nullptr, a.norm, L, S, g.indy, 0, ty, lane);
   } else if (warp == 1) {
-    if (a.qb) {
-      load_col(L, a.qb + co, n, lane);
-      warp_line_transform(L, S, g.indy, 0, ty, lane);
-      for (int j = lane; j <= n; j += 32) L[j] *= a.norm;
-    } else {
+    if (a.qb)
+      line_transform<P>(a.qb + co, nullptr, a.norm, L, S, g.indy, 0, ty, lane);
+    else
       for (int j = lane; j <= n; j += 32) L[j] = 0.f;
-    }
   }
   __syncthreads();
   // phase 2: the solves of the slice start, mode by mode
@@ -103,39 +93,33 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
       case 6: dst = a.out_bx; par = 1; break;
       default: dst = a.out_by; par = 0; break;
     }
-    __syncwarp();
-    warp_line_transform(L, S, g.indy, par, ty, lane);
-    store_col(dst + co, L, n, lane, 1.f);
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, lane);
+    line_store(dst + co, L, n, 1.f, lane);
   }
 }
 
-__global__ void __launch_bounds__(256) k_slice_b(SliceB b, GridDims g, KCoef K, LineTables ty,
+// 9 warps: warps 0-7 carry the 8 transformed components, warp 8 the optional
+// cbq line (q + cu_z).
+template <int P>
+__global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, LineTables ty,
                                                  DevStatus* st) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   if (st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = g.ny, npad = n + 6;
+  const int n = g.ny, pitch = col_pitch(n);
   const int kx = blockIdx.x;
   const long long co = (long long)kx * g.kp;
   float* line[9];
 #pragma unroll
-  for (int w = 0; w < 8; ++w) line[w] = smem + 2 * w * npad;
-  line[8] = smem + 16 * npad;
-  float* L = line[warp];
-  float* S = L + npad;
+  for (int w = 0; w < 9; ++w) line[w] = smem + w * pitch;
+  float* L = smem + warp * pitch;
+  float* S = smem + (9 + warp) * pitch;
   // phase 1: forward y of cu(3), dcu(2), amu(3): y parities S C S, S C, S S C
-  {
+  if (warp < 8) {
     const int par = (warp == 1 || warp == 4 || warp == 7) ? 1 : 0;
-    load_col(L, b.in[warp] + co, n, lane);
-    warp_line_transform(L, S, g.indy, par, ty, lane);
-    for (int j = lane; j <= n; j += 32) L[j] *= b.norm;
-    if (warp == 0 && b.q_in) {
-      __syncwarp();
-      float* Lq = line[8];
-      load_col(Lq, b.q_in + co, n, lane);
-      warp_line_transform(Lq, S, g.indy, 0, ty, lane);
-      for (int j = lane; j <= n; j += 32) Lq[j] *= b.norm;
-    }
+    line_transform<P>(b.in[warp] + co, nullptr, b.norm, L, S, g.indy, par, ty, lane);
+  } else if (b.q_in) {
+    line_transform<P>(b.q_in + co, nullptr, b.norm, L, S, g.indy, 0, ty, lane);
   }
   __syncthreads();
   // phase 2: corrector, extrapolated current, psit and bxyz of the next pass
@@ -177,46 +161,60 @@ __global__ void __launch_bounds__(256) k_slice_b(SliceB b, GridDims g, KCoef K, 
   // phase 3: inverse y of psit (S), bx (C), by (S), bz (C) and the smoothed q (S)
   if (warp < 4) {
     const int par = (warp == 1 || warp == 3) ? 1 : 0;
-    warp_line_transform(L, S, g.indy, par, ty, lane);
-    store_col(b.out[warp] + co, L, n, lane, 1.f);
-  } else if (warp == 4 && b.q_in) {
-    float* Lq = line[8];
-    warp_line_transform(Lq, S, g.indy, 0, ty, lane);
-    store_col(b.q_out + co, Lq, n, lane, 1.f);
-  } else if (warp >= 5 && b.nzero) {
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, lane);
+    line_store(b.out[warp] + co, L, n, 1.f, lane);
+  } else if (warp == 8) {
+    if (b.q_in) {
+      line_transform<P>(L, nullptr, 1.f, L, S, g.indy, 0, ty, lane);
+      line_store(b.q_out + co, L, n, 1.f, lane);
+    }
+  } else if (b.nzero) {
     // zero the real-space accumulators for the next pass (their values were
     // consumed by the x pass that precedes this kernel)
     const long long per = (g.rplane + gridDim.x - 1) / gridDim.x;
     const long long lo = per * kx, hi = min(g.rplane, lo + per);
     for (int z = 0; z < b.nzero; ++z)
-      for (long long i = lo + (threadIdx.x - 160); i < hi; i += 96) b.zero[z][i] = 0.f;
+      for (long long i = lo + (threadIdx.x - 128); i < hi; i += 128) b.zero[z][i] = 0.f;
   }
 }
 
 }  // namespace
 
-size_t slice_a_smem(const GridDims& g) { return sizeof(float) * 16 * (size_t)(g.ny + 6); }
-size_t slice_b_smem(const GridDims& g) { return sizeof(float) * 17 * (size_t)(g.ny + 6); }
+size_t slice_a_smem(const GridDims& g) {
+  return sizeof(float) * (g.indy < 6 ? 16 : 8) * (size_t)col_pitch(g.ny);
+}
+size_t slice_b_smem(const GridDims& g) {
+  return sizeof(float) * (g.indy < 6 ? 18 : 9) * (size_t)col_pitch(g.ny);
+}
+
+template <int P>
+static int set_slice_smem(int big) {
+  if (cudaFuncSetAttribute(k_slice_a<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_slice_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
+          cudaSuccess)
+    return -2;
+  return 0;
+}
 
 int slice_kernels_init() {
-  const int big = (int)(sizeof(float) * 17 * ((1 << QP_MAX_IND) + 6));
-  if (cudaFuncSetAttribute(k_slice_a, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
-      cudaSuccess)
-    return -2;
-  if (cudaFuncSetAttribute(k_slice_b, cudaFuncAttributeMaxDynamicSharedMemorySize, big) !=
-      cudaSuccess)
-    return -2;
+  const int big = (int)(sizeof(float) * 9 * col_pitch(1 << QP_MAX_IND));
+  for (int logn = 4; logn <= QP_MAX_IND; ++logn) {
+    int rc = 0;
+    QP_LINE_SWITCH(logn, rc = set_slice_smem<P_>(big));
+    if (rc) return rc;
+  }
   return 0;
 }
 
 void launch_slice_a(const SliceA& a, const GridDims& g, const KCoef& K, const LineTables& ty,
                     const DevStatus* st, cudaStream_t s) {
-  k_slice_a<<<g.nx + 1, 256, slice_a_smem(g), s>>>(a, g, K, ty, st);
+  QP_LINE_SWITCH(g.indy, (k_slice_a<P_><<<g.nx + 1, 256, slice_a_smem(g), s>>>(a, g, K, ty, st)));
 }
 
 void launch_slice_b(const SliceB& b, const GridDims& g, const KCoef& K, const LineTables& ty,
                     DevStatus* st, cudaStream_t s) {
-  k_slice_b<<<g.nx + 1, 256, slice_b_smem(g), s>>>(b, g, K, ty, st);
+  QP_LINE_SWITCH(g.indy, (k_slice_b<P_><<<g.nx + 1, 288, slice_b_smem(g), s>>>(b, g, K, ty, st)));
 }
 
 }  // namespace qp
