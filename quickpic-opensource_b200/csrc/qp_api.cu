@@ -129,10 +129,21 @@ static int ensure_staging(qp_ctx* ctx, size_t bytes) {
   return 0;
 }
 
+// Zero freshly allocated device memory before anything else can touch it.
+// The contexts' streams are non-blocking, so a memset left pending on the
+// legacy default stream could land after later work on a context stream.
+static int zero_now(void* p, size_t bytes) {
+  if (cudaMemset(p, 0, bytes) != cudaSuccess) return -1;
+  return cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess ? 0 : -1;
+}
+
 static float* dalloc(size_t n, bool zero = true) {
   float* p = nullptr;
   if (cudaMalloc(&p, sizeof(float) * std::max<size_t>(n, 1)) != cudaSuccess) return nullptr;
-  if (zero) cudaMemset(p, 0, sizeof(float) * std::max<size_t>(n, 1));
+  if (zero && zero_now(p, sizeof(float) * std::max<size_t>(n, 1))) {
+    cudaFree(p);
+    return nullptr;
+  }
   return p;
 }
 
@@ -184,7 +195,7 @@ extern "C" int qp_ctx_create(const qp_grid_desc* grid, int device, qp_ctx** out)
   ctx->tg.ntiles = ctx->tg.mx1 * ctx->tg.myp1;
   ctx->tg.rp = ctx->g.rp;
   CK(cudaMalloc(&ctx->st, sizeof(DevStatus)));
-  CK(cudaMemset(ctx->st, 0, sizeof(DevStatus)));
+  if (zero_now(ctx->st, sizeof(DevStatus))) return fail(ctx, __LINE__, "status set-up failed");
   CK(cudaDeviceSynchronize());
   *out = ctx;
   return 0;
@@ -587,8 +598,7 @@ static int part_alloc(PartBuf* P, int ntiles, int cap) {
     if (!P->c[c]) return -1;
   }
   if (cudaMalloc(&P->count, sizeof(int) * ntiles) != cudaSuccess) return -1;
-  cudaMemset(P->count, 0, sizeof(int) * ntiles);
-  return 0;
+  return zero_now(P->count, sizeof(int) * ntiles);
 }
 
 static void part_free(PartBuf* P) {
@@ -607,8 +617,7 @@ static int inbox_alloc(Inbox* ib, int ntiles, int cap) {
   if (cudaMalloc(&ib->key, sizeof(unsigned long long) * (size_t)ntiles * cap) != cudaSuccess)
     return -1;
   if (cudaMalloc(&ib->count, sizeof(int) * ntiles) != cudaSuccess) return -1;
-  cudaMemset(ib->count, 0, sizeof(int) * ntiles);
-  return 0;
+  return zero_now(ib->count, sizeof(int) * ntiles);
 }
 
 static void inbox_free(Inbox* ib) {

@@ -56,6 +56,15 @@ void line_tables_free(LineTablesHost* t) {
 }
 
 // ------------------------------------------------------------------ x pass
+// The slice cursor must name one of the planes of the 3D array a component
+// reads or writes; otherwise the launch raises an error and does nothing.
+__device__ __forceinline__ bool cursor_ok(const XComp& c, const DevStatus* st) {
+  const int cur = st->cursor;
+  if (cur >= 0 && cur < c.cursor_planes) return true;
+  if (threadIdx.x == 0) atomicCAS(const_cast<int*>(&st->error), 0, -7);
+  return false;
+}
+
 // Shared memory of the line kernels: 8 lines of pitch n + 4 floats (16-byte
 // aligned rows; the transposed accesses below hit 32 distinct banks), plus 8
 // scratch lines for lines shorter than 64 points.
@@ -78,7 +87,10 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
   const int y0 = blockIdx.x * 8;
   const int y = y0 + warp;
   long long cur = 0;
-  if (c.cursor_stride) cur = (long long)st->cursor * c.cursor_stride;
+  if (c.cursor_stride) {
+    if (!cursor_ok(c, st)) return;
+    cur = (long long)st->cursor * c.cursor_stride;
+  }
   if (y <= g.ny) {
     const float* s1 = c.src + cur + (long long)y * g.rp;
     const float* s2 = c.src2 ? c.src2 + (long long)y * g.rp : nullptr;
@@ -103,6 +115,7 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   const int n = g.nx, pitch = line_pitch(n);
   if (st && st->error) return;
   const XComp c = job.c[blockIdx.y];
+  if (c.cursor_stride && !cursor_ok(c, st)) return;
   const int y0 = blockIdx.x * 8;
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
     const int r = idx & 7, kx = idx >> 3;

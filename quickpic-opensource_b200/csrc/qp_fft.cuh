@@ -27,6 +27,7 @@ struct XComp {
   float scale;
   int parity;  // 0 sine, 1 cosine
   long long cursor_stride;
+  int cursor_planes;  // planes of that 3D array: a cursor outside them raises an error
 };
 struct XJob {
   XComp c[QP_MAX_JOB];

@@ -161,10 +161,15 @@ __global__ void k_kscale(GridDims g, float* p, float v, const DevStatus* st) {
 // updated in place as in the reference.
 __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by, const float* bz,
                           const float* psit, Planes3 be, Planes3 bb, float dex, int store,
-                          float* zero_q, DevStatus* st) {
+                          int nplanes, float* zero_q, DevStatus* st) {
   if (st->error) return;
+  const int cur = st->cursor;
+  if (store && (cur < 0 || cur >= nplanes)) {  // never store outside the 3D arrays
+    if (threadIdx.x == 0) atomicCAS(&st->error, 0, -7);
+    return;
+  }
   const long long n = g.rplane;
-  const long long pl = (long long)st->cursor * g.rplane;
+  const long long pl = (long long)cur * g.rplane;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     float f1 = -1.f * fx[i], f2 = -1.f * fy[i];
@@ -256,12 +261,12 @@ void launch_kscale(const GridDims& g, float* p, float v, const DevStatus* st, cu
 void launch_cursor(DevStatus* st, int v, cudaStream_t s) { k_cursor<<<1, 1, 0, s>>>(st, v); }
 
 void launch_store3d(const GridDims& g, float* const* fxy, float* const* bxyz, const float* psit,
-                    const Planes3& be, const Planes3& bb, float dex, int store, float* zero_q,
-                    DevStatus* st, cudaStream_t s) {
+                    const Planes3& be, const Planes3& bb, float dex, int store, int nplanes,
+                    float* zero_q, DevStatus* st, cudaStream_t s) {
   long long blocks = (g.rplane + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_store3d<<<(int)blocks, 256, 0, s>>>(g, fxy[0], fxy[1], bxyz[0], bxyz[1], bxyz[2], psit, be,
-                                        bb, dex, store, zero_q, st);
+                                        bb, dex, store, nplanes, zero_q, st);
 }
 
 }  // namespace qp

@@ -27,7 +27,7 @@ void launch_kscale(const GridDims& g, float* p, float v, const DevStatus* st, cu
 void launch_cursor(DevStatus* st, int v, cudaStream_t s);
 // also clears zero_q (if not null) and advances the slice cursor
 void launch_store3d(const GridDims& g, float* const* fxy, float* const* bxyz, const float* psit,
-                    const Planes3& be, const Planes3& bb, float dex, int store, float* zero_q,
-                    DevStatus* st, cudaStream_t s);
+                    const Planes3& be, const Planes3& bb, float dex, int store, int nplanes,
+                    float* zero_q, DevStatus* st, cudaStream_t s);
 
 }  // namespace qp

@@ -71,6 +71,10 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
   tile_origin(tg, t, &noffp, &moffp);
   __syncthreads();
   const int n = P.count[t];
+  if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
   const long long base = (long long)t * P.cap;
   for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
     const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
@@ -138,6 +142,10 @@ __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const fl
   __syncthreads();
   const float dx2 = dex * dex;
   const int n = P.count[t];
+  if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
   const long long base = (long long)t * P.cap;
   for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
     const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
@@ -280,6 +288,10 @@ __global__ void __launch_bounds__(256) k_amjdp(PartBuf P, TileGeom tg, GatherPla
   const float dti = 1.f / dt;
   const float idex = 1.f / dex;
   const int n = P.count[t];
+  if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
   const long long base = (long long)t * P.cap;
   for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
     const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
@@ -397,6 +409,10 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   const float edgelx = (float)noffp, edgerx = (float)(noffp + TILE);
   const float edgely = (float)moffp, edgery = (float)(moffp + TILE);
   const int n = A.count[t];
+  if (n < 0 || n > A.cap) {  // a count beyond the tile's slots: never read past them
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
   const long long base = (long long)t * A.cap;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r0 = 0; r0 < n; r0 += blockDim.x) {
@@ -544,6 +560,10 @@ __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg
     return;
   }
   const int stay = B.count[t];
+  if (stay < 0 || stay > B.cap) {
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
   if (stay + nin > B.cap) {
     raise_error(st, QP_OVERFLOW);
     atomicMax(&st->need_cap, stay + nin);
