@@ -157,7 +157,7 @@ def make_engine(qpgpu, cfg, device):
         beams.append(qpgpu.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
                                   peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                   center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
-    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=True)
+    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False)
     return ctx, sp, beams, sim
 
 

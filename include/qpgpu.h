@@ -234,9 +234,11 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
 
 /* The whole 3D step of go_simulation (simulation_class.f03:611-764) for the
  * species and beams given, with all state on the GPU: beam deposit, the
- * per-slice loop (643-736) captured as CUDA graphs, and the species renew.
+ * per-slice loop (643-736) as one fixed sequence of kernel launches per
+ * slice, and the species renew.
  * iter = fixed number of B predictor-corrector passes (simulation.iter);
- * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3. */
+ * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
+ * use_graphs is accepted and ignored: the slices are launched directly. */
 typedef struct {
   int iter;
   int store3d;

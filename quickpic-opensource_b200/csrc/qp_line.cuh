@@ -292,7 +292,10 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
         z[i] = make_float2(A.x + B.x, A.y + B.y);
         float2 D = make_float2(A.x - B.x, A.y - B.y);
         const int k = (i & (s - 1)) * (16 / s);
-        if (k) D = cmul(D, t.tw[k * P]);
+        if (k == 8)
+          D = make_float2(D.y, -D.x);  // exp(-2 pi i 8 / 32) = -i
+        else if (k)
+          D = cmul(D, t.tw[k * P]);
         z[i + s] = D;
       }
     }
@@ -303,17 +306,22 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
   // 4. twiddle exp(-2 pi i lane k2 / (n/2))
 #pragma unroll
   for (int k2 = 1; k2 < P; ++k2) w[k2] = cmul(w[k2], t.tw[lane * k2]);
-  // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles)
+  // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles): the lower
+  //    lane of a pair keeps v + p, the upper one (p - v) * twiddle; written as
+  //    fma(sign, v, p) times a twiddle that is 1 on the lower lanes (and on
+  //    every lane in the last stage)
 #pragma unroll
   for (int s = 16; s >= 1; s >>= 1) {
     const bool hi = (lane & s) != 0;
-    const float2 tws = hi ? t.tw[(lane & (s - 1)) * (16 / s) * P] : make_float2(1.f, 0.f);
+    const float sg = hi ? -1.f : 1.f;
+    const float2 tws =
+        (hi && s > 1) ? t.tw[(lane & (s - 1)) * (16 / s) * P] : make_float2(1.f, 0.f);
 #pragma unroll
     for (int k2 = 0; k2 < P; ++k2) {
       const float2 v = w[k2];
       const float2 p = shfl_xor2(v, s);
-      const float2 d = hi ? make_float2(p.x - v.x, p.y - v.y) : make_float2(v.x + p.x, v.y + p.y);
-      w[k2] = hi ? cmul(d, tws) : d;
+      const float2 d = make_float2(fmaf(sg, v.x, p.x), fmaf(sg, v.y, p.y));
+      w[k2] = (s > 1) ? cmul(d, tws) : d;
     }
   }
   // 6. real-FFT unscramble: Y[k] = sum_j y[j] exp(-2 pi i j k / n), k = k2 + P k1

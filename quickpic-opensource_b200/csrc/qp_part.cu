@@ -598,7 +598,12 @@ __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg
   }
   const long long ob = (long long)t * B.cap + stay;
   for (int i = threadIdx.x; i < nin; i += blockDim.x) {
-    const long long src = ib0 + sidx[i];
+    const int si = sidx[i];
+    if (si < 0 || si >= nin) {  // the sort must map the first nin keys onto filled slots
+      raise_error(st, -8);
+      continue;
+    }
+    const long long src = ib0 + si;
 #pragma unroll
     for (int c = 0; c < NCOMP; ++c) B.c[c][ob + i] = ib.c[c][src];
   }

@@ -402,7 +402,7 @@ class Beam3d:
 class Simulation:
     """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
 
-    def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=True):
+    def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False):
         d = _SimDesc()
         d.iter = iter
         d.store3d = 1 if store3d else 0
