@@ -248,6 +248,39 @@ def run_engine(args, cfg, rank, world, local_rank, dist):
                 beam_np=int(sum(np.prod(b["np"]) for b in cfg["beams"])))
 
 
+def run_fft_case(args, cfg):
+    """Kernel case: class-level fftrk + fftkr (kind 2) of a 3-component field on the
+    workload's transverse grid; one step = one round trip.  Deterministic and
+    free of particles, so the transform kernels can be profiled on their own."""
+    import qpgpu
+
+    g = cfg["grid"]
+    ctx = qpgpu.Context(g["ind"][0], g["ind"][1], 1, g["box"])
+    f = qpgpu.Field2d(ctx, 3)
+    rng = np.random.default_rng(1)
+    f.set_rs(rng.standard_normal(ctx.rs_shape(3)).astype(np.float32))
+    for _ in range(args.warmup):
+        f.fftrk(2)
+        f.fftkr(2)
+    ctx.sync()
+    import torch
+
+    torch.cuda.profiler.start()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        f.fftrk(2)
+        f.fftkr(2)
+    ms = ctx.timer_stop()
+    torch.cuda.profiler.stop()
+    nx, ny = 1 << g["ind"][0], 1 << g["ind"][1]
+    byts = 3 * 4.0 * (nx + 1) * (ny + 1) * 2 * 2 * args.steps  # 3 comps, 2 passes each way
+    print(json.dumps({"case": "fft", "grid": [nx, ny], "components": 3, "steps": args.steps,
+                      "us_per_round_trip": 1e3 * ms / args.steps,
+                      "algorithmic_GBps": byts / (ms * 1e-3) / 1e9}), flush=True)
+    f.close()
+    ctx.close()
+
+
 def max_over_ranks(v, dist):
     if dist is None:
         return v
@@ -331,8 +364,13 @@ def main():
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", default="step", choices=["step", "fft"],
+                    help="step: the 3D step (the benchmark); fft: transform kernels alone")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if args.case == "fft":
+        run_fft_case(args, cfg)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

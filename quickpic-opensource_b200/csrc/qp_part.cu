@@ -265,7 +265,7 @@ __device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, 
 // atomics about 4x and spreads a warp's atomics over different cells.
 // The per-particle products are those of the reference; only the order in
 // which a node's contributions are summed differs.
-__global__ void __launch_bounds__(256) k_amjdp(PartBuf P, TileGeom tg, GatherPlanes f,
+__global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, GatherPlanes f,
                                                float* cux, float* cuy, float* cuz, float* dcx,
                                                float* dcy, float* amxx, float* amyy,
                                                float* amxy, float qbm, float dt, float dex,
