@@ -6,7 +6,8 @@ plasma with 2 x 2 particles per cell (the reference loader gives
 510 * 511 * 4 = 1,042,440 FP32 electrons), tri-Gaussian drive beam of
 256 x 256 x 128 = 8,388,608 macro-particles, sigma_r = 0.3, sigma_z = 0.6 c/wp,
 nb/np = 4, gamma = 20000 with 1% energy spread and normalised emittance 0.01.
-A step is one 3D step: beam deposit, all 512 slices, species renew.
+A step is one 3D step: beam deposit, all 512 slices, the beam push with the
+step's 3D fields (dt = 10 / omega_p), species renew.
 Inputs are synthetic (seeded loaders of the reference, no dataset).
 
 metric: plasma particle-slices/s = (plasma particles x slices) / device time.
@@ -40,21 +41,21 @@ BOX = [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]]
 
 CONFIGS = {
     # the plain-method medium case (512^3, 4 ppc, 8.4M beam particles)
-    "medium": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2,
+    "medium": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2, dt=10.0,
                    species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
                    beams=[dict(np=[256, 256, 128], q=-1.0, m=1.0, gamma=20000.0,
                                peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                                sigma=[0.3, 0.3, 0.6],
                                sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the medium transverse grid with 64 slices: the profiling case (< 1 GB on the device)
-    "prof": dict(grid=dict(ind=[9, 9, 6], box=BOX), iter=2,
+    "prof": dict(grid=dict(ind=[9, 9, 6], box=BOX), iter=2, dt=10.0,
                  species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
                  beams=[dict(np=[256, 256, 16], q=-1.0, m=1.0, gamma=20000.0,
                              peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                              sigma=[0.3, 0.3, 0.6],
                              sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the small CPU-runnable case (128^3, 2x2 ppc, 262,144 beam particles)
-    "small": dict(grid=dict(ind=[7, 7, 7], box=BOX), iter=2,
+    "small": dict(grid=dict(ind=[7, 7, 7], box=BOX), iter=2, dt=10.0,
                   species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
                   beams=[dict(np=[64, 64, 64], q=-1.0, m=1.0, gamma=20000.0,
                               peak_density=2.0, quiet_start=True, center=[0.0, 0.0, 2.5],
@@ -157,7 +158,8 @@ def make_engine(qpgpu, cfg, device):
         beams.append(qpgpu.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
                                   peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                   center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
-    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False)
+    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False,
+                           dt=cfg.get("dt", 0.0))
     return ctx, sp, beams, sim
 
 
@@ -321,7 +323,8 @@ def workload_desc(cfg, name):
     return (f"{name}: {1 << g[0]}x{1 << g[1]} transverse, {1 << g[2]} slices, "
             f"{cfg['species']['ppc'][0]}x{cfg['species']['ppc'][1]} ppc, beam "
             f"{int(np.prod(b['np']))} particles sigma_r={b['sigma'][0]} sigma_z={b['sigma'][2]} "
-            f"nb/np={b['peak_density']}, iter={cfg['iter']} (fixed predictor-corrector passes)")
+            f"nb/np={b['peak_density']}, iter={cfg['iter']} (fixed predictor-corrector passes), "
+            f"beam push dt={cfg.get('dt', 0.0)}")
 
 
 def run_reference(args, cfg):

@@ -224,9 +224,9 @@ int qp_beam_qdp(qp_beam* b);
  * (1-based) of the beam's 3D charge; q must be in state 0. */
 int qp_beam_qdpcopy(qp_beam* b, qp_field2d* q, int slice);
 int qp_beam_download(qp_beam* b, float* part /* (7, np) */);
-/* Replace the beam's particles with part(7, np) from host memory (np must
- * equal qp_beam_np); the restart read of beam particles, part3d%rrst
- * (part3d_class.f03:315-331), without the HDF5 file. */
+/* Replace the beam's particles with part(7, np) from host memory (np at most
+ * the particle count the beam was created with); the restart read of beam
+ * particles, part3d%rrst (part3d_class.f03:315-331), without the HDF5 file. */
 int qp_beam_upload(qp_beam* b, const float* part, long long np);
 int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
 
@@ -238,12 +238,16 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * slice, and the species renew.
  * iter = fixed number of B predictor-corrector passes (simulation.iter);
  * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
- * use_graphs is accepted and ignored: the slices are launched directly. */
+ * use_graphs is accepted and ignored: the slices are launched directly;
+ * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
+ * step with beam3d%push of every beam with the stored bexyz, bbxyz
+ * (simulation_class.f03:753-757), dt = 0 leaves the beams where they are. */
 typedef struct {
   int iter;
   int store3d;
   int use_graphs;
-  int reserved[5];
+  float dt;
+  int reserved[4];
 } qp_sim_desc;
 
 typedef struct {
@@ -257,6 +261,13 @@ typedef struct {
 int qp_sim_create(qp_ctx* ctx, const qp_sim_desc* d, qp_species* const* species, int nspecies,
                   qp_beam* const* beams, int nbeams, qp_sim** out);
 int qp_sim_destroy(qp_sim* sim);
+/* beam3d%push (beam3d_class.f03:155-180 -> part3d%partpush, PGBPUSH32L_QP,
+ * part3d_lib77.f:630-786) of beam b with the 3D fields bexyz, bbxyz of the
+ * last step of `sim` (store3d = 1) and time step dt.  Conducting boundaries:
+ * a particle that leaves [1, n-1) cells in x, y or z is dropped; the
+ * remaining ones keep their order.  With one pipeline stage part3d%pmove
+ * (PMOVE32) has nothing to move, so this is the whole beam3d%push. */
+int qp_beam_push(qp_beam* b, qp_sim* sim, float dt);
 /* One 3D step; `stats` may be NULL.  The species are renewed at the end. */
 int qp_sim_step3d(qp_sim* sim, qp_step_stats* stats);
 /* Fields of the last slice (real space or Fourier space, reference layout):

@@ -260,6 +260,17 @@ def beam_deposit(part, ind3, dtype=np.float32):
     return q3
 
 
+def beam_push(part, fxyz, bxyz, qbm, dt, dex, dxi, ind3, dtype=np.float32):
+    """PGBPUSH32L_QP on part(7, np) with 3D fields (3, nx+2, ny+1, nz+1); returns the
+    pushed particles, (7, np_new), after conducting-boundary drops."""
+    p = np.array(part, dtype=dtype, order="F", copy=True)
+    fe = np.asfortranarray(fxyz, dtype=dtype)
+    fb = np.asfortranarray(bxyz, dtype=dtype)
+    n = _call("oq_pgbpush32l_qp", dtype, p, p.shape[1], fe, fb, float(qbm), float(dt),
+              float(dex), float(dxi), ind3[0], ind3[1], ind3[2])
+    return p[:, :n]
+
+
 # -------------------------------------------------------------- simulation
 P_FIXED = 20
 B_NPAR = 18
@@ -284,6 +295,7 @@ def sim_params(cfg) -> np.ndarray:
     p[15] = sp.get("xtras", 0.2)
     p[16] = len(cfg["beams"])
     p[17] = 1 if cfg.get("store3d", True) else 0
+    p[18] = cfg.get("dt", 0.0)  # 3D time step; > 0 pushes the beams after the slices
     for b, bm in enumerate(cfg["beams"]):
         o = P_FIXED + B_NPAR * b
         p[o:o + 3] = bm["np"]

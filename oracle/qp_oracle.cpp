@@ -1506,6 +1506,102 @@ int prvdist32_random(T* part, int npmax, int* npp, T qm, T vtx, T vty, T vtz, T 
   return ierr;
 }
 
+// PGBPUSH32L_QP, part3d_lib77.f:630-786 (one partition, noff = 0): the
+// quasi-static beam push with the 3D fields of the step.  fxyz and bxyz are
+// (3, nxv, nypmx, nzpmx); only the first two components of bxyz are used.
+// With ipbc = 1 (conducting, the only solver, spect2d_class.f03:19) a particle
+// that leaves [1, n-1) in x, y or z is dropped: the last particle takes its
+// slot and is pushed in its place, as the reference does.  Returns the new
+// particle count.
+template <class T>
+int pgbpush32l_qp(T* part, int npp, const T* fxyz, const T* bxyz, T qbm, T dt, T dtc, int nx,
+                  int ny, int nz, int nxv, int nypmx, int ipbc, T deltax, T deltaz, T cofd) {
+  const T qtmh = qbm * dt;
+  const T dtcx = dtc / deltax;
+  const T dtcz = dtc / deltaz;
+  const T cofd1 = cofd / dt;
+  T edgelx = T(0), edgely = T(0), edgelz = T(0), edgerx = T(0), edgery = T(0), edgerz = T(0);
+  if (ipbc == 1) {
+    edgelx = edgely = edgelz = T(1.);
+    edgerx = T(nx - 1);
+    edgery = T(ny - 1);
+    edgerz = T(nz - 1);
+  }
+  const int mnoff = -1, lnoff = -1;
+#define F3(a, c, b, l)                                                                   \
+  a[(size_t)((c)-1) +                                                                  \
+    3 * ((size_t)((b)-1) + (size_t)nxv * ((size_t)((l)-1) + (size_t)nypmx * (size_t)(lz - 1)))]
+  int inpp = npp;
+  int j = 1;
+  while (j <= inpp) {
+    T* p = &part[7 * (size_t)(j - 1)];
+    int nn = (int)p[0], mm = (int)p[1], lz = (int)p[2];
+    T dxp = p[0] - T(nn);
+    T dyp = p[1] - T(mm);
+    T dzp = p[2] - T(lz);
+    nn = nn + 1;
+    T amx = T(1.) - dxp;
+    T amy = T(1.) - dyp;
+    const int np = nn + 1;
+    mm = mm - mnoff;
+    T dx1 = dxp * dyp;
+    dyp = amx * dyp;
+    const int mp = mm + 1;
+    amx = amx * amy;
+    T amz = T(1.) - dzp;
+    lz = lz - lnoff;
+    amy = dxp * amy;
+    // trilinear gather of component c of field a at (nn..np, mm..mp, lz..lz+1)
+    auto tri = [&](const T* a, int c) {
+      T lo = amx * F3(a, c, nn, mm) + amy * F3(a, c, np, mm) + dyp * F3(a, c, nn, mp) +
+             dx1 * F3(a, c, np, mp);
+      ++lz;
+      T hi = amx * F3(a, c, nn, mm) + amy * F3(a, c, np, mm) + dyp * F3(a, c, nn, mp) +
+             dx1 * F3(a, c, np, mp);
+      --lz;
+      return amz * lo + dzp * hi;
+    };
+    T dx = tri(fxyz, 1), dy = tri(fxyz, 2), dz = tri(fxyz, 3);
+    const T ox = tri(bxyz, 1), oy = tri(bxyz, 2);
+    dx = dx - oy;
+    dy = dy + ox;
+    const T delx = qtmh * dx, dely = qtmh * dy, delz = qtmh * dz;
+    dx = p[3] + delx;
+    dy = p[4] + dely;
+    dz = p[5] + delz;
+    p[3] = dx;
+    p[4] = dy;
+    const T p2t = dx * dx + dy * dy;
+    const T p2l = dz * dz;
+    const T p2 = p2t + p2l;
+    const T ngamma = std::sqrt(T(1.) + p2);
+    const T dtgx = dtcx / ngamma;
+    const T dtgy = dtcx / ngamma;
+    const T one_minus_vz = (T(1.) + p2t) / (dz * (dz + ngamma));
+    dz = dz - cofd1 * ngamma * ((delx * delx + dely * dely) * dz - delz * (delx * dx + dely * dy));
+    p[5] = dz;
+    dx = p[0] + dx * dtgx;
+    dy = p[1] + dy * dtgy;
+    dz = p[2] + one_minus_vz * dtcz;
+    if (ipbc == 1 && (dx < edgelx || dx >= edgerx || dy < edgely || dy >= edgery ||
+                      dz < edgelz || dz >= edgerz)) {
+      if (j == inpp) {
+        --inpp;
+        break;
+      }
+      std::copy(&part[7 * (size_t)(inpp - 1)], &part[7 * (size_t)inpp], p);
+      --inpp;
+      continue;  // push the particle moved into slot j
+    }
+    p[0] = dx;
+    p[1] = dy;
+    p[2] = dz;
+    ++j;
+  }
+#undef F3
+  return inpp;
+}
+
 // PGPOST32L, part3d_lib77.f:554-628 (one partition, noff = 0)
 template <class T>
 void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
@@ -1660,6 +1756,13 @@ void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
     return prvdist32_random<T>(part, npmax, npp, qm, vtx, vty, vtz, T(0), T(0), vdz,    \
                                npx, npy, npz, 1 << indx, 1 << indy, 1 << indz, sigx,    \
                                sigy, sigz, x0, y0, z0, cx, cy, quiet != 0);             \
+  }                                                                                     \
+  extern "C" int oq_pgbpush32l_qp_##S(T* part, int npp, const T* fxyz, const T* bxyz,  \
+                                      T qbm, T dt, T dex, T dxi, int indx, int indy,    \
+                                      int indz) {                                       \
+    return pgbpush32l_qp<T>(part, npp, fxyz, bxyz, qbm, dt, dt, 1 << indx, 1 << indy,   \
+                            1 << indz, (1 << indx) + 2, (1 << indy) + 1, 1, dex, dxi,   \
+                            T(0));                                                      \
   }                                                                                     \
   extern "C" int oq_pgpost32l_##S(const T* part, int npp, T* q3, int indx, int indy,    \
                                   int indz) {                                           \

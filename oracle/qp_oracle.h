@@ -87,6 +87,10 @@ extern "C" {
                               int indy, int indz, T sigx, T sigy, T sigz, T x0,     \
                               T y0, T z0, const T* cx, const T* cy, int quiet);     \
   int oq_pgpost32l_##S(const T* part, int npp, T* q3, int indx, int indy, int indz);\
+  /* beam push PGBPUSH32L_QP with the 3D fields (3, nx+2, ny+1, nz+1); conducting  \
+     boundaries drop particles; returns the new count */                             \
+  int oq_pgbpush32l_qp_##S(T* part, int npp, const T* fxyz, const T* bxyz, T qbm,   \
+                           T dt, T dex, T dxi, int indx, int indy, int indz);        \
   /* full simulation driver (simulation_class.f03:593-769) */                        \
   void* oq_sim_create_##S(const T* params, int nparams);                            \
   int oq_sim_destroy_##S(void* h);                                                   \

@@ -99,6 +99,9 @@ struct qp_beam {
   qp_ctx* ctx;
   BeamBuf b{};
   float* q3d = nullptr;  // (nz+1) real planes
+  float qbm = 0.f;       // charge-to-mass ratio q/m of the push
+  long long cap = 0;     // particle slots of each plane (the count at creation)
+  int* keep = nullptr;   // per-particle flags of the push (allocated by the first push)
 };
 
 // ------------------------------------------------------------ helpers
@@ -1044,6 +1047,8 @@ extern "C" int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out)
   qp_beam* b = new qp_beam();
   b->ctx = ctx;
   b->b.np = n;
+  b->cap = n;
+  b->qbm = d->q / d->m;
   for (int k = 0; k < BCOMP; ++k) {
     b->b.c[k] = dalloc(n, false);
     if (!b->b.c[k]) return fail(ctx, __LINE__, "out of device memory");
@@ -1060,6 +1065,7 @@ extern "C" int qp_beam_destroy(qp_beam* b) {
   cudaStreamSynchronize(b->ctx->stream);
   for (int k = 0; k < BCOMP; ++k) cudaFree(b->b.c[k]);
   cudaFree(b->q3d);
+  if (b->keep) cudaFree(b->keep);
   delete b;
   return 0;
 }
@@ -1094,7 +1100,10 @@ extern "C" int qp_beam_qdpcopy(qp_beam* b, qp_field2d* q, int slice) {
 
 extern "C" int qp_beam_upload(qp_beam* b, const float* part, long long np) {
   qp_ctx* ctx = b->ctx;
-  if (np != b->b.np) return fail(ctx, __LINE__, "beam upload: particle count differs");
+  if (np < 0 || np > b->cap)
+    return fail(ctx, __LINE__, "beam upload: more particles than the beam holds (" +
+                                   std::to_string(b->cap) + ")");
+  b->b.np = np;
   if (ensure_staging(ctx, sizeof(float) * 7 * (size_t)np)) return -1;
   CK(cudaMemcpyAsync(ctx->staging, part, sizeof(float) * 7 * (size_t)np, cudaMemcpyHostToDevice,
                      ctx->stream));

@@ -58,7 +58,8 @@ struct DevStatus {
   int need_inbox;     // movers a tile must accept
   int cursor;         // slice cursor of the fused 3D step
   int iter_done;      // iterations run in the current slice
-  int pad[2];         // pad[0]: CTA completion counter of the store kernel
+  int store_ctas;     // CTA completion counter of the 3D store kernel
+  int beam_drops;     // beam particles dropped at the conducting boundary
   float resid_num;    // convergence residual accumulators
   float resid_den;
 };

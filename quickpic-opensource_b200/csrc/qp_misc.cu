@@ -196,9 +196,9 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    const int done = atomicAdd(&st->pad[0], 1);
+    const int done = atomicAdd(&st->store_ctas, 1);
     if (done == (int)gridDim.x - 1) {
-      st->pad[0] = 0;
+      st->store_ctas = 0;
       st->cursor = st->cursor + 1;
       __threadfence();
     }

@@ -96,7 +96,7 @@ class _BeamDesc(C.Structure):
 
 class _SimDesc(C.Structure):
     _fields_ = [("iter", C.c_int), ("store3d", C.c_int), ("use_graphs", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("dt", C.c_float), ("reserved", C.c_int * 4)]
 
 
 class StepStats(C.Structure):
@@ -376,6 +376,10 @@ class Beam3d:
         else:
             self.ctx._check(self.ctx._L.qp_beam_qdpcopy(self.h, q.h, slice))
 
+    def push(self, sim, dt):
+        """beam3d%push with the 3D fields of `sim`'s last step (conducting boundaries)."""
+        self.ctx._check(self.ctx._L.qp_beam_push(self.h, sim.h, C.c_float(dt)))
+
     def get_particles(self):
         out = np.zeros((7, self.np()), dtype=np.float32, order="F")
         self.ctx._check(self.ctx._L.qp_beam_download(self.h, _ptr(out)))
@@ -402,11 +406,13 @@ class Beam3d:
 class Simulation:
     """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
 
-    def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False):
+    def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False,
+                 dt=0.0):
         d = _SimDesc()
         d.iter = iter
         d.store3d = 1 if store3d else 0
         d.use_graphs = 1 if use_graphs else 0
+        d.dt = dt  # 3D time step; > 0 ends every step with the beam push
         sp = (C.c_void_p * len(species))(*[s.h for s in species])
         bm = (C.c_void_p * max(len(beams), 1))(*[b.h for b in beams])
         h = C.c_void_p()

@@ -326,7 +326,7 @@ def test_beam_loader_and_deposit(qp, ctx, oracle_mod):
     bm.close()
 
 
-def _gpu_sim(qp, cfg, use_graphs=False):
+def _gpu_sim(qp, cfg, use_graphs=False, dt=0.0):
     ind = cfg["grid"]["ind"]
     c = qp.Context(ind[0], ind[1], ind[2], cfg["grid"]["box"])
     s = cfg["species"]
@@ -337,7 +337,8 @@ def _gpu_sim(qp, cfg, use_graphs=False):
         beams.append(qp.Beam3d(c, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
                                peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
-    sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs)
+    sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs,
+                        dt=dt)
     return c, sp, beams, sim
 
 
@@ -386,4 +387,82 @@ def test_full_3d_step_matches_oracle(qp, oracle_mod, use_graphs=False):
         assert rel_l2(sim.get_field(name), o64.get(name).reshape(sim.get_field(name).shape,
                                                                  order="F")) < 1e-3, name
     sim.close()
+    c.close()
+
+
+def _sorted_cols(p):
+    return p[:, np.lexsort(p[::-1])]
+
+
+def test_beam_push_matches_oracle(qp, oracle_mod):
+    """beam3d%push (PGBPUSH32L_QP) on the 3D fields of a GPU step, against the
+    oracle push of the same particles and fields: bit-exact per particle.
+    Six particles are moved next to the x and z boundaries with momenta that
+    carry them out, so the conducting-boundary drop and the compaction run;
+    the engine keeps the survivors in order, the reference fills holes from the
+    end, so the particle sets are compared."""
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 5))
+    ind = cfg["grid"]["ind"]
+    c, sp, beams, sim = _gpu_sim(qp, cfg)
+    sim.step3d()
+    bm = beams[0]
+    pre = bm.get_particles()
+    nx, nz = 1 << ind[0], 1 << ind[2]
+    for i, (x, z, px, pz) in enumerate([(nx - 1.02, None, 50.0, None), (1.01, None, -50.0, None),
+                                        (nx - 1.5, None, 0.0, None), (None, nz - 1.0001, None, 1.0),
+                                        (None, 1.0001, None, None), (nx - 1.0001, None, 10.0, None)]):
+        j = 100 + 37 * i
+        if x is not None:
+            pre[0, j] = x
+        if z is not None:
+            pre[2, j] = z
+        if px is not None:
+            pre[3, j] = px
+        if pz is not None:
+            pre[5, j] = pz
+    bm.set_particles(pre)
+    be, bb = sim.get_3d("bexyz"), sim.get_3d("bbxyz")
+    dex = (cfg["grid"]["box"][0][1] - cfg["grid"]["box"][0][0]) / nx
+    dxi = (cfg["grid"]["box"][2][1] - cfg["grid"]["box"][2][0]) / nz
+    dt = 10.0
+    bm.push(sim, dt)
+    got = bm.get_particles()
+    exp = O.beam_push(pre, be, bb, -1.0 / 1.0, dt, np.float32(dex), np.float32(dxi), ind)
+    assert exp.shape[1] < pre.shape[1], "the test expects some particles to be dropped"
+    assert got.shape == exp.shape
+    assert np.array_equal(_sorted_cols(got), _sorted_cols(exp))
+    # the survivors keep their order: push each particle alone and keep those that stay
+    one = [O.beam_push(pre[:, [j]], be, bb, -1.0, dt, np.float32(dex), np.float32(dxi), ind)
+           for j in range(pre.shape[1])]
+    stable = np.concatenate([o for o in one if o.shape[1]], axis=1)
+    assert np.array_equal(got, stable)
+    sim.close()
+    bm.close()
+    sp.close()
+    c.close()
+
+
+def test_step_with_beam_push(qp, oracle_mod):
+    """A 3D step with dt > 0 ends with the beam push: the beam after the step
+    equals the oracle push of the beam before it with the step's 3D fields."""
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 5))
+    ind = cfg["grid"]["ind"]
+    nx, nz = 1 << ind[0], 1 << ind[2]
+    c, sp, beams, sim = _gpu_sim(qp, cfg, dt=10.0)
+    bm = beams[0]
+    pre = bm.get_particles()
+    st = sim.step3d()
+    got = bm.get_particles()
+    be, bb = sim.get_3d("bexyz"), sim.get_3d("bbxyz")
+    dex = (cfg["grid"]["box"][0][1] - cfg["grid"]["box"][0][0]) / nx
+    dxi = (cfg["grid"]["box"][2][1] - cfg["grid"]["box"][2][0]) / nz
+    exp = O.beam_push(pre, be, bb, -1.0, 10.0, np.float32(dex), np.float32(dxi), ind)
+    assert got.shape == exp.shape
+    assert np.array_equal(_sorted_cols(got), _sorted_cols(exp))
+    assert np.abs(got[3] - pre[3]).max() > 0  # the beam did move
+    sim.close()
+    bm.close()
+    sp.close()
     c.close()

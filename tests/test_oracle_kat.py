@@ -206,3 +206,29 @@ def test_fp32_oracle_tracks_fp64(oracle_mod):
         e = rel_l2(s32.get(name), s64.get(name))
         assert e < 1e-4, (name, e)
     assert np.abs(s64.get("psi")).max() > 1e-3  # the beam drove a wake
+
+
+def test_beam_push_free_streaming_and_drop(oracle_mod):
+    """PGBPUSH32L_QP with zero fields: momenta unchanged, x += px dt/(dex gamma),
+    z += (1 + p_perp^2) / (pz (pz + gamma)) dt/dxi; a particle that crosses
+    x >= nx - 1 is dropped and the last particle takes its slot."""
+    O = oracle_mod
+    ind = (5, 5, 4)
+    nx, ny, nz = 32, 32, 16
+    fe = np.zeros((3, nx + 2, ny + 1, nz + 1), dtype=np.float64, order="F")
+    fb = np.zeros_like(fe)
+    part = np.zeros((7, 3), dtype=np.float64, order="F")
+    part[:, 0] = [10.5, 12.25, 8.5, 0.3, -0.2, 200.0, 1.0]
+    part[:, 1] = [nx - 1.01, 12.0, 8.0, 50.0, 0.0, 100.0, 1.0]   # leaves through x
+    part[:, 2] = [5.0, 6.0, 7.0, -0.1, 0.4, 300.0, 1.0]
+    dt, dex, dxi = 10.0, 0.375, 0.625
+    out = O.beam_push(part, fe, fb, -1.0, dt, dex, dxi, ind, dtype=np.float64)
+    assert out.shape == (7, 2)
+    for k, src in ((0, 0), (1, 2)):   # particle 2 moved into the hole at slot 1
+        px, py, pz = part[3:6, src]
+        g = np.sqrt(1.0 + px * px + py * py + pz * pz)
+        assert np.allclose(out[3:6, k], part[3:6, src], rtol=0, atol=0)
+        assert np.isclose(out[0, k], part[0, src] + px * dt / dex / g, rtol=1e-14)
+        assert np.isclose(out[1, k], part[1, src] + py * dt / dex / g, rtol=1e-14)
+        dzc = (1.0 + px * px + py * py) / (pz * (pz + g)) * dt / dxi
+        assert np.isclose(out[2, k], part[2, src] + dzc, rtol=1e-14)
