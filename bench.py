@@ -200,8 +200,7 @@ def run_engine(args, cfg, rank, world, local_rank, dist):
     torch.cuda.profiler.stop()
     clocks.stop()
     barrier()
-    t_ms = max_over_ranks(t_ms, dist)
-    value = npl * nz * args.steps * world / (t_ms * 1e-3)
+    value, t_ms = job_throughput(float(npl * nz * args.steps), t_ms, dist)
 
     # ---- e2e: beam in from pinned host memory, wake lineout out, every step
     bm = beams[0]
@@ -218,8 +217,8 @@ def run_engine(args, cfg, rank, world, local_rank, dist):
         sim.lineout(3, out=line)
     e_ms = ctx.timer_stop()
     barrier()
-    e_ms = max_over_ranks(e_ms, dist)
-    e2e = {"value": npl * nz * args.steps * world / (e_ms * 1e-3), "unit": "particle-slices/s",
+    e_val, e_ms = job_throughput(float(npl * nz * args.steps), e_ms, dist)
+    e2e = {"value": e_val, "unit": "particle-slices/s",
            "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(line.nbytes),
            "ms_per_step": e_ms / args.steps}
 
@@ -283,14 +282,31 @@ def run_fft_case(args, cfg):
     ctx.close()
 
 
-def max_over_ranks(v, dist):
+def _reduce(v, dist, op):
     if dist is None:
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op(dist))
     return float(t.item())
+
+
+def max_over_ranks(v, dist):
+    return _reduce(v, dist, lambda d: d.ReduceOp.MAX)
+
+
+def sum_over_ranks(v, dist):
+    return _reduce(v, dist, lambda d: d.ReduceOp.SUM)
+
+
+def job_throughput(units_local, t_ms_local, dist):
+    """Whole-job throughput of independent replicas: the units every rank
+    processed over the slowest rank's device time.  Returns (units/s, max ms)."""
+    t_ms = max_over_ranks(t_ms_local, dist)
+    units = sum_over_ranks(units_local, dist)
+    return units / (t_ms * 1e-3), t_ms
 
 
 def cpu_slices(cfg, budget_s, max_slices, threads):
