@@ -802,7 +802,7 @@ extern "C" int qp_species_extpsi(qp_species* sp, qp_field2d* psi, float dex) {
 }
 
 static GatherPlanes gplanes(qp_field2d* fxy, qp_field2d* bxyz, qp_field2d* psit, int combine) {
-  GatherPlanes f;
+  GatherPlanes f{};
   f.fx = fxy->rs[0];
   f.fy = fxy->rs[1];
   f.bx = bxyz->rs[0];

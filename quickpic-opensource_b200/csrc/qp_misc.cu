@@ -168,29 +168,41 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
     if (threadIdx.x == 0) atomicCAS(&st->error, 0, -7);
     return;
   }
-  const long long n = g.rplane;
-  const long long pl = (long long)cur * g.rplane;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+  // four nodes per thread: planes and rows are 16-byte aligned (rp = nx + 4)
+  const long long n4 = g.rplane >> 2;
+  const long long pl4 = (long long)cur * n4;
+  float4* fx4 = reinterpret_cast<float4*>(fx);
+  float4* fy4 = reinterpret_cast<float4*>(fy);
+  float4* bx4 = reinterpret_cast<float4*>(bx);
+  float4* by4 = reinterpret_cast<float4*>(by);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
        i += (long long)gridDim.x * blockDim.x) {
-    float f1 = -1.f * fx[i], f2 = -1.f * fy[i];
-    f1 = f1 + by[i];
-    f2 = f2 - bx[i];
-    f1 = f1 * dex;
-    f2 = f2 * dex;
-    fx[i] = f1;
-    fy[i] = f2;
-    const float b1 = bx[i] * dex, b2 = by[i] * dex;
-    bx[i] = b1;
-    by[i] = b2;
+    const float4 vfx = fx4[i], vfy = fy4[i], vbx = bx4[i], vby = by4[i];
+    float4 f1, f2, b1, b2;
+    // f1 = (-fx + by) * dex, f2 = (-fy - bx) * dex; b1 = bx * dex, b2 = by * dex
+    f1.x = (-1.f * vfx.x + vby.x) * dex;
+    f1.y = (-1.f * vfx.y + vby.y) * dex;
+    f1.z = (-1.f * vfx.z + vby.z) * dex;
+    f1.w = (-1.f * vfx.w + vby.w) * dex;
+    f2.x = (-1.f * vfy.x - vbx.x) * dex;
+    f2.y = (-1.f * vfy.y - vbx.y) * dex;
+    f2.z = (-1.f * vfy.z - vbx.z) * dex;
+    f2.w = (-1.f * vfy.w - vbx.w) * dex;
+    b1 = make_float4(vbx.x * dex, vbx.y * dex, vbx.z * dex, vbx.w * dex);
+    b2 = make_float4(vby.x * dex, vby.y * dex, vby.z * dex, vby.w * dex);
+    fx4[i] = f1;
+    fy4[i] = f2;
+    bx4[i] = b1;
+    by4[i] = b2;
     if (store) {
-      be.p[0][pl + i] = f1;
-      be.p[1][pl + i] = f2;
-      be.p[2][pl + i] = psit[i];
-      bb.p[0][pl + i] = b1;
-      bb.p[1][pl + i] = b2;
-      bb.p[2][pl + i] = bz[i];
+      reinterpret_cast<float4*>(be.p[0])[pl4 + i] = f1;
+      reinterpret_cast<float4*>(be.p[1])[pl4 + i] = f2;
+      reinterpret_cast<float4*>(be.p[2])[pl4 + i] = reinterpret_cast<const float4*>(psit)[i];
+      reinterpret_cast<float4*>(bb.p[0])[pl4 + i] = b1;
+      reinterpret_cast<float4*>(bb.p[1])[pl4 + i] = b2;
+      reinterpret_cast<float4*>(bb.p[2])[pl4 + i] = reinterpret_cast<const float4*>(bz)[i];
     }
-    if (zero_q) zero_q[i] = 0.f;  // species charge plane, ready for the next deposit
+    if (zero_q) reinterpret_cast<float4*>(zero_q)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   // the last CTA to finish advances the slice cursor
   __syncthreads();
@@ -263,7 +275,7 @@ void launch_cursor(DevStatus* st, int v, cudaStream_t s) { k_cursor<<<1, 1, 0, s
 void launch_store3d(const GridDims& g, float* const* fxy, float* const* bxyz, const float* psit,
                     const Planes3& be, const Planes3& bb, float dex, int store, int nplanes,
                     float* zero_q, DevStatus* st, cudaStream_t s) {
-  long long blocks = (g.rplane + 255) / 256;
+  long long blocks = ((g.rplane >> 2) + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_store3d<<<(int)blocks, 256, 0, s>>>(g, fxy[0], fxy[1], bxyz[0], bxyz[1], bxyz[2], psit, be,
                                         bb, dex, store, nplanes, zero_q, st);

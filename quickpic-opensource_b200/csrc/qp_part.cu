@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
                                                float* dcy, float* amxx, float* amyy,
                                                float* amxy, float qbm, float dt, float dex,
                                                float scale, DevStatus* st) {
-  __shared__ float sf[6][TN * TN];
+  __shared__ float sf[7][TN * TN];
   __shared__ float sa[8][TN * TN];
   if (st && st->error) return;
   const int t = blockIdx.x;
@@ -282,11 +282,14 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   stage(sf[3], f.by, tg, noffp, moffp);
   stage(sf[4], f.bz, tg, noffp, moffp);
   stage(sf[5], f.psit, tg, noffp, moffp);
+  const bool ext = f.psi != nullptr;
+  if (ext) stage(sf[6], f.psi, tg, noffp, moffp);
   for (int i = threadIdx.x; i < 8 * TN * TN; i += blockDim.x) (&sa[0][0])[i] = 0.f;
   __syncthreads();
   const float qtmh = 0.5f * qbm * dt;
   const float dti = 1.f / dt;
   const float idex = 1.f / dex;
+  const float dx2 = dex * dex;
   const int n = P.count[t];
   if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
     if (threadIdx.x == 0) raise_error(st, -6);
@@ -298,12 +301,16 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
     const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + base + k0);
     const float4 VX = *reinterpret_cast<const float4*>(P.c[2] + base + k0);
     const float4 VY = *reinterpret_cast<const float4*>(P.c[3] + base + k0);
-    float4 P6 = *reinterpret_cast<const float4*>(P.c[5] + base + k0);
-    const float4 P7 = *reinterpret_cast<const float4*>(P.c[6] + base + k0);
+    // with ext, p6 and p7 are formed here from psi (k_extpsi) instead of read
+    float4 P6 = make_float4(0.f, 0.f, 0.f, 0.f), P7 = P6;
+    if (!ext) {
+      P6 = *reinterpret_cast<const float4*>(P.c[5] + base + k0);
+      P7 = *reinterpret_cast<const float4*>(P.c[6] + base + k0);
+    }
     const float4 QM = *reinterpret_cast<const float4*>(P.c[7] + base + k0);
     const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
     const float vxs[4] = {VX.x, VX.y, VX.z, VX.w}, vys[4] = {VY.x, VY.y, VY.z, VY.w};
-    const float p6s[4] = {P6.x, P6.y, P6.z, P6.w}, p7s[4] = {P7.x, P7.y, P7.z, P7.w};
+    float p6s[4] = {P6.x, P6.y, P6.z, P6.w}, p7s[4] = {P7.x, P7.y, P7.z, P7.w};
     const float qms[4] = {QM.x, QM.y, QM.z, QM.w};
     float p6o[4] = {P6.x, P6.y, P6.z, P6.w};
     float acc[8][4];
@@ -318,6 +325,15 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
         if (nn < 0 || nn >= TILE || mm < 0 || mm >= TILE) {
           raise_error(st, -3);
           continue;
+        }
+        if (ext) {
+          // WPGPSIPOST2L_QP for this particle, the same arithmetic as k_extpsi
+          float d = gather(sf[6], nn, mm, 1.f - dxp, 1.f - dyp, dxp, dyp);
+          d = -d * dx2 * qbm;
+          p7s[j] = 1.f + d;
+          p6s[j] = d + (dx2 * (vxs[j] * vxs[j] + vys[j] * vys[j]) - d * d - 2.f * d) /
+                           (2.f * (1.f + d)) +
+                   1.f;
         }
         AmjOut o;
         amjdp_one(sf, nn, mm, dxp, dyp, vxs[j], vys[j], p6s[j], p7s[j], qms[j], qbm, qtmh, dti,
@@ -358,6 +374,8 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
     }
     P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
     *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
+    if (ext)
+      *reinterpret_cast<float4*>(P.c[6] + base + k0) = make_float4(p7s[0], p7s[1], p7s[2], p7s[3]);
   }
   __syncthreads();
   flush(sa[0], cux, tg, noffp, moffp, scale);

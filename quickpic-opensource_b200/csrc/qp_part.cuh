@@ -39,6 +39,7 @@ struct GatherPlanes {
   const float* bz;   // bxyz(3)
   const float* psit; // psit
   int combine;       // 1: the push uses -fxy + (by, -bx), the final slice force
+  const float* psi;  // amjdp only, optional: form p6, p7 from psi first (extpsi)
 };
 
 int part_kernels_init();
