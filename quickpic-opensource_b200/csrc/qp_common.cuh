@@ -48,7 +48,22 @@ struct LineTables {
   const float* cs;   // cos(pi j / n), j = 0..n
   const float2* tw;  // exp(-2 pi i m / (n/2)), m = 0..n/2-1  (complex FFT of n/2)
   const float2* uw;  // exp(-2 pi i k / n),     k = 0..n/2    (real-FFT unscramble)
+  // n >= 64: the same values rearranged as the register transform reads them,
+  // one row of 32 per register slot (qp_line.cuh, LT_*), lane_floats floats
+  const float* lane;
+  int lane_floats;
 };
+
+// Layout of LineTables::lane for P = n / 64 (offsets in floats).
+__host__ __device__ constexpr int lt_sn0(int P) { return 0; }
+__host__ __device__ constexpr int lt_sn1(int P) { return 32 * P; }
+__host__ __device__ constexpr int lt_cs0(int P) { return 64 * P; }
+__host__ __device__ constexpr int lt_cs1(int P) { return 96 * P; }
+__host__ __device__ constexpr int lt_tw4(int P) { return 128 * P; }   // float2 [P][32]
+__host__ __device__ constexpr int lt_uw(int P) { return 192 * P; }    // float2 [P][32]
+__host__ __device__ constexpr int lt_tw5(int P) { return 256 * P; }   // float2 [4][32]
+__host__ __device__ constexpr int lt_tw3(int P) { return 256 * P + 256; }  // float2 [16]
+__host__ __device__ constexpr int lt_floats(int P) { return P > 0 ? 256 * P + 288 : 0; }
 
 // Sticky device status shared by every kernel of a context.
 struct DevStatus {

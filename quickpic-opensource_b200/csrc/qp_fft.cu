@@ -7,6 +7,7 @@
 // fftkr (field2d_class.f03:193-227) = the unnormalised y pass, then the x pass
 // reading [kx][y] and writing rows, then the guard copy row ny = row 0
 // (ufield2d copyguard, ufield2d_lib.f03:37-42) done by the CTA owning row 0.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -28,7 +29,43 @@ int line_tables_build(LineTablesHost* t, int logn) {
     tw[m] = make_float2((float)std::cos(-2.0 * pi * m / h), (float)std::sin(-2.0 * pi * m / h));
   for (int k = 0; k <= h; ++k)
     uw[k] = make_float2((float)std::cos(-2.0 * pi * k / n), (float)std::sin(-2.0 * pi * k / n));
-  size_t bytes = sizeof(float) * 2 * (n + 1) + sizeof(float2) * (2 * h + 1) + 64;
+  // the per-lane rearrangement for the register transform (n >= 64)
+  const int P = n >= 64 ? n / 64 : 0;
+  std::vector<float> lt(lt_floats(P), 0.f);
+  if (P > 0) {
+    auto f2 = [&](int off, int i, float2 v) {
+      lt[off + 2 * i] = v.x;
+      lt[off + 2 * i + 1] = v.y;
+    };
+    auto brev5 = [](int v) {
+      int r = 0;
+      for (int b = 0; b < 5; ++b)
+        if (v >> b & 1) r |= 1 << (4 - b);
+      return r;
+    };
+    for (int a = 0; a < P; ++a)
+      for (int l = 0; l < 32; ++l) {
+        const int m = l + 32 * a, j0 = 2 * m, j1 = 2 * m + 1;
+        lt[lt_sn0(P) + 32 * a + l] = sn[std::min(j0, n - j0)];
+        lt[lt_sn1(P) + 32 * a + l] = sn[std::min(j1, n - j1)];
+        lt[lt_cs0(P) + 32 * a + l] = cs[j0];
+        lt[lt_cs1(P) + 32 * a + l] = cs[j1];
+      }
+    for (int k2 = 0; k2 < P; ++k2)
+      for (int l = 0; l < 32; ++l) {
+        f2(lt_tw4(P), 32 * k2 + l, tw[l * k2]);
+        f2(lt_uw(P), 32 * k2 + l, uw[k2 + P * brev5(l)]);
+      }
+    for (int si = 0; si < 4; ++si) {
+      const int st = 16 >> si;
+      for (int l = 0; l < 32; ++l)
+        f2(lt_tw5(P), 32 * si + l,
+           (l & st) ? tw[(l & (st - 1)) * (16 / st) * P] : make_float2(1.f, 0.f));
+    }
+    for (int k = 0; k < 16; ++k) f2(lt_tw3(P), k, tw[k * P]);
+  }
+  size_t bytes = sizeof(float) * 2 * (n + 1) + sizeof(float2) * (2 * h + 1) + 64 +
+                 sizeof(float) * lt.size() + 16;
   char* d = nullptr;
   if (cudaMalloc(&d, bytes) != cudaSuccess) return -2;
   float* dsn = reinterpret_cast<float*>(d);
@@ -41,6 +78,16 @@ int line_tables_build(LineTablesHost* t, int logn) {
   cudaMemcpy(dtw, tw.data(), sizeof(float2) * h, cudaMemcpyHostToDevice);
   if (cudaMemcpy(duw, uw.data(), sizeof(float2) * (h + 1), cudaMemcpyHostToDevice) != cudaSuccess)
     return -2;
+  float* dlt = nullptr;
+  if (P > 0) {
+    const size_t lo = ((size_t)(reinterpret_cast<char*>(duw + h + 1) - d) + 15) & ~size_t(15);
+    dlt = reinterpret_cast<float*>(d + lo);
+    if (cudaMemcpy(dlt, lt.data(), sizeof(float) * lt.size(), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return -2;
+  }
+  t->t.lane = dlt;
+  t->t.lane_floats = (int)lt.size();
   t->base = d;
   t->t.sn = dsn;
   t->t.cs = dcs;
@@ -91,10 +138,15 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
     if (!cursor_ok(c, st)) return;
     cur = (long long)st->cursor * c.cursor_stride;
   }
+  float* T = smem + line_count(g.indx) * pitch;
+  if (P > 0) {
+    stage_lane_table(T, tx);
+    __syncthreads();
+  }
   if (y <= g.ny) {
     const float* s1 = c.src + cur + (long long)y * g.rp;
     const float* s2 = c.src2 ? c.src2 + (long long)y * g.rp : nullptr;
-    line_transform<P>(s1, s2, c.scale, L, S, g.indx, c.parity, tx, lane);
+    line_transform<P>(s1, s2, c.scale, L, S, g.indx, c.parity, tx, T, lane);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
@@ -117,6 +169,8 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   const XComp c = job.c[blockIdx.y];
   if (c.cursor_stride && !cursor_ok(c, st)) return;
   const int y0 = blockIdx.x * 8;
+  float* T = smem + line_count(g.indx) * pitch;
+  if (P > 0) stage_lane_table(T, tx);  // covered by the barrier after the gather
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
     const int r = idx & 7, kx = idx >> 3;
     const int yy = y0 + r;
@@ -127,7 +181,7 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   float* S = smem + (8 + warp) * pitch;
   const int y = y0 + warp;
   if (y < g.ny) {
-    line_transform<P>(L, nullptr, 1.f, L, S, g.indx, c.parity, tx, lane);
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indx, c.parity, tx, T, lane);
     long long cur = 0;
     if (c.cursor_stride) cur = (long long)st->cursor * c.cursor_stride;
     float* d = c.dst + cur + (long long)y * g.rp;
@@ -156,21 +210,26 @@ __global__ void __launch_bounds__(256) k_ycol(YJob job, GridDims g, LineTables t
   const int n = g.ny, pitch = line_pitch(n);
   float* L = smem + warp * pitch;
   float* S = smem + (8 + warp) * pitch;
+  float* T = smem + line_count(g.indy) * pitch;
+  if (P > 0) {
+    stage_lane_table(T, ty);
+    __syncthreads();
+  }
   const int kx = blockIdx.x * 8 + warp;
   if (kx > g.nx) return;
   for (int ci = 0; ci < job.ncomp; ++ci) {
     float* col = job.c[ci].plane + (long long)kx * g.kp;
-    line_transform<P>(col, nullptr, 1.f, L, S, g.indy, job.c[ci].parity, ty, lane);
+    line_transform<P>(col, nullptr, 1.f, L, S, g.indy, job.c[ci].parity, ty, T, lane);
     line_store(col, L, n, job.c[ci].scale, lane);
     __syncwarp();
   }
 }
 
 size_t xpass_smem(const GridDims& g) {
-  return sizeof(float) * line_count(g.indx) * (size_t)line_pitch(g.nx);
+  return sizeof(float) * ((size_t)line_count(g.indx) * line_pitch(g.nx) + lt_floats(line_p(g.indx)));
 }
 size_t ypass_smem(const GridDims& g) {
-  return sizeof(float) * line_count(g.indy) * (size_t)line_pitch(g.ny);
+  return sizeof(float) * ((size_t)line_count(g.indy) * line_pitch(g.ny) + lt_floats(line_p(g.indy)));
 }
 
 template <int P>
@@ -186,7 +245,8 @@ static int set_smem_limits(int big) {
 }
 
 int fft_kernels_init() {
-  const int big = (int)(sizeof(float) * 8 * line_pitch(1 << QP_MAX_IND));
+  const int big = (int)(sizeof(float) * (8 * line_pitch(1 << QP_MAX_IND) +
+                                         lt_floats(line_p(QP_MAX_IND))));
   for (int logn = 4; logn <= QP_MAX_IND; ++logn) {
     int rc = 0;
     QP_LINE_SWITCH(logn, rc = set_smem_limits<P_>(big));

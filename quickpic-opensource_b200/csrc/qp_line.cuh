@@ -224,7 +224,12 @@ __device__ __forceinline__ float2 shfl2(float2 v, int src) {
 // `in` and `in2` may point to global or shared memory, 8-byte aligned.
 template <int P>
 __device__ __forceinline__ void reg_line(const float* in, const float* in2, float in_scale,
-                                         float* out, int parity, const LineTables& t, int lane) {
+                                         float* out, int parity, const float* T, int lane) {
+  // T: the lane table of this line length staged in shared memory (lt_* layout)
+  const float2* tw3 = reinterpret_cast<const float2*>(T + lt_tw3(P));
+  const float2* tw4 = reinterpret_cast<const float2*>(T + lt_tw4(P));
+  const float2* tw5 = reinterpret_cast<const float2*>(T + lt_tw5(P));
+  const float2* uwl = reinterpret_cast<const float2*>(T + lt_uw(P));
   constexpr int N = 64 * P;
   const unsigned FULL = 0xffffffffu;
   // 1. the line: x[2m], x[2m+1] for m = lane + 32 a, and x[n]
@@ -254,8 +259,8 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
 #pragma unroll
     for (int a = 0; a < P; ++a) {
       const int j = 2 * (lane + 32 * a);
-      if (j) acc += xp[a].x * t.cs[j];
-      acc += xp[a].y * t.cs[j + 1];
+      if (j) acc += xp[a].x * T[lt_cs0(P) + 32 * a + lane];
+      acc += xp[a].y * T[lt_cs1(P) + 32 * a + lane];
     }
     acc = warp_sum(acc);
     sigma = __shfl_sync(FULL, 0.5f * (xp[0].x - xn), 0) + acc;
@@ -268,8 +273,7 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
     float r0 = __shfl_sync(FULL, xp[P - 1 - a].x, (32 - lane) & 31);  // x[n - 2m]
     if (lane == 0) r0 = (a == 0) ? xn : xp[(P - a) % P].x;
     const float r1 = __shfl_xor_sync(FULL, xp[P - 1 - a].y, 31);  // x[n - 2m - 1]
-    const int j0 = 2 * m, j1 = 2 * m + 1;
-    const float s0 = t.sn[min(j0, N - j0)], s1 = t.sn[min(j1, N - j1)];
+    const float s0 = T[lt_sn0(P) + 32 * a + lane], s1 = T[lt_sn1(P) + 32 * a + lane];
     const float x0 = xp[a].x, x1 = xp[a].y;
     float y0, y1;
     if (parity == 0) {
@@ -295,7 +299,7 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
         if (k == 8)
           D = make_float2(D.y, -D.x);  // exp(-2 pi i 8 / 32) = -i
         else if (k)
-          D = cmul(D, t.tw[k * P]);
+          D = cmul(D, tw3[k]);
         z[i + s] = D;
       }
     }
@@ -305,7 +309,7 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
   for (int k2 = 0; k2 < P; ++k2) w[k2] = z[brev_p<P>(k2)];
   // 4. twiddle exp(-2 pi i lane k2 / (n/2))
 #pragma unroll
-  for (int k2 = 1; k2 < P; ++k2) w[k2] = cmul(w[k2], t.tw[lane * k2]);
+  for (int k2 = 1; k2 < P; ++k2) w[k2] = cmul(w[k2], tw4[32 * k2 + lane]);
   // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles): the lower
   //    lane of a pair keeps v + p, the upper one (p - v) * twiddle; written as
   //    fma(sign, v, p) times a twiddle that is 1 on the lower lanes (and on
@@ -314,8 +318,9 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
   for (int s = 16; s >= 1; s >>= 1) {
     const bool hi = (lane & s) != 0;
     const float sg = hi ? -1.f : 1.f;
-    const float2 tws =
-        (hi && s > 1) ? t.tw[(lane & (s - 1)) * (16 / s) * P] : make_float2(1.f, 0.f);
+    // the table holds (1, 0) for the lower lanes of each stage
+    const int si = (s == 16) ? 0 : (s == 8) ? 1 : (s == 4) ? 2 : 3;
+    const float2 tws = (s > 1) ? tw5[32 * si + lane] : make_float2(1.f, 0.f);
 #pragma unroll
     for (int k2 = 0; k2 < P; ++k2) {
       const float2 v = w[k2];
@@ -343,7 +348,7 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
     } else {
       const float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y + B.y));
       const float2 D = make_float2(A.x - B.x, A.y - B.y);
-      const float2 q = cmul(t.uw[k], D);
+      const float2 q = cmul(uwl[32 * k2 + lane], D);
       Y = make_float2(E.x + 0.5f * q.y, E.y - 0.5f * q.x);
     }
     // sine:   out[2k] = -2 Im Y[k], out[2k+1] = Re Y[0] + 2 sum_{m=1..k} Re Y[m]
@@ -393,9 +398,9 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
 template <int P>
 __device__ __forceinline__ void line_transform(const float* in, const float* in2, float in_scale,
                                                float* sline, float* sscr, int logn, int parity,
-                                               const LineTables& t, int lane) {
+                                               const LineTables& t, const float* T, int lane) {
   if constexpr (P > 0) {
-    reg_line<P>(in, in2, in_scale, sline, parity, t, lane);
+    reg_line<P>(in, in2, in_scale, sline, parity, T, lane);
   } else {
     const int n = 1 << logn;
     float v[2];
@@ -427,6 +432,14 @@ constexpr int line_p(int logn) { return logn < 6 ? 0 : 1 << (logn - 6); }
     case 11: { constexpr int P_ = 32; STMT; } break; \
     default: { constexpr int P_ = 0; STMT; } break;  \
   }
+
+// Copy the lane table of a line length into shared memory (all threads of the
+// block; the caller synchronises before the first transform).
+__device__ __forceinline__ void stage_lane_table(float* T, const LineTables& t) {
+  const float4* src = reinterpret_cast<const float4*>(t.lane);
+  float4* dst = reinterpret_cast<float4*>(T);
+  for (int i = threadIdx.x; i < (t.lane_floats >> 2); i += blockDim.x) dst[i] = __ldg(src + i);
+}
 
 // Coalesced copy of a shared line (n + 1 floats) to global memory, times sc.
 __device__ __forceinline__ void line_store(float* dst, const float* sline, int n, float sc,

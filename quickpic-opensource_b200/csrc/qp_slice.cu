@@ -45,12 +45,17 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   for (int w = 0; w < 8; ++w) line[w] = smem + w * pitch;
   float* L = smem + warp * pitch;
   float* S = smem + (8 + warp) * pitch;
+  float* T = smem + (P > 0 ? 8 : 16) * pitch;
+  if (P > 0) {
+    stage_lane_table(T, ty);
+    __syncthreads();
+  }
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
   if (warp == 0) {
-    line_transform<P>(a.qe + co, nullptr, a.norm, L, S, g.indy, 0, ty, lane);
+    line_transform<P>(a.qe + co, nullptr, a.norm, L, S, g.indy, 0, ty, T, lane);
   } else if (warp == 1) {
     if (a.qb)
-      line_transform<P>(a.qb + co, nullptr, a.norm, L, S, g.indy, 0, ty, lane);
+      line_transform<P>(a.qb + co, nullptr, a.norm, L, S, g.indy, 0, ty, T, lane);
     else
       for (int j = lane; j <= n; j += 32) L[j] = 0.f;
   }
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
       case 6: dst = a.out_bx; par = 1; break;
       default: dst = a.out_by; par = 0; break;
     }
-    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, lane);
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, T, lane);
     line_store(dst + co, L, n, 1.f, lane);
   }
 }
@@ -114,12 +119,17 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
   for (int w = 0; w < 9; ++w) line[w] = smem + w * pitch;
   float* L = smem + warp * pitch;
   float* S = smem + (9 + warp) * pitch;
+  float* T = smem + (P > 0 ? 9 : 18) * pitch;
+  if (P > 0) {
+    stage_lane_table(T, ty);
+    __syncthreads();
+  }
   // phase 1: forward y of cu(3), dcu(2), amu(3): y parities S C S, S C, S S C
   if (warp < 8) {
     const int par = (warp == 1 || warp == 4 || warp == 7) ? 1 : 0;
-    line_transform<P>(b.in[warp] + co, nullptr, b.norm, L, S, g.indy, par, ty, lane);
+    line_transform<P>(b.in[warp] + co, nullptr, b.norm, L, S, g.indy, par, ty, T, lane);
   } else if (b.q_in) {
-    line_transform<P>(b.q_in + co, nullptr, b.norm, L, S, g.indy, 0, ty, lane);
+    line_transform<P>(b.q_in + co, nullptr, b.norm, L, S, g.indy, 0, ty, T, lane);
   }
   __syncthreads();
   // phase 2: corrector, extrapolated current, psit and bxyz of the next pass
@@ -161,11 +171,11 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
   // phase 3: inverse y of psit (S), bx (C), by (S), bz (C) and the smoothed q (S)
   if (warp < 4) {
     const int par = (warp == 1 || warp == 3) ? 1 : 0;
-    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, lane);
+    line_transform<P>(L, nullptr, 1.f, L, S, g.indy, par, ty, T, lane);
     line_store(b.out[warp] + co, L, n, 1.f, lane);
   } else if (warp == 8) {
     if (b.q_in) {
-      line_transform<P>(L, nullptr, 1.f, L, S, g.indy, 0, ty, lane);
+      line_transform<P>(L, nullptr, 1.f, L, S, g.indy, 0, ty, T, lane);
       line_store(b.q_out + co, L, n, 1.f, lane);
     }
   } else if (b.nzero) {
@@ -181,10 +191,12 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
 }  // namespace
 
 size_t slice_a_smem(const GridDims& g) {
-  return sizeof(float) * (g.indy < 6 ? 16 : 8) * (size_t)col_pitch(g.ny);
+  return sizeof(float) *
+         ((g.indy < 6 ? 16 : 8) * (size_t)col_pitch(g.ny) + lt_floats(line_p(g.indy)));
 }
 size_t slice_b_smem(const GridDims& g) {
-  return sizeof(float) * (g.indy < 6 ? 18 : 9) * (size_t)col_pitch(g.ny);
+  return sizeof(float) *
+         ((g.indy < 6 ? 18 : 9) * (size_t)col_pitch(g.ny) + lt_floats(line_p(g.indy)));
 }
 
 template <int P>
@@ -198,7 +210,8 @@ static int set_slice_smem(int big) {
 }
 
 int slice_kernels_init() {
-  const int big = (int)(sizeof(float) * 9 * col_pitch(1 << QP_MAX_IND));
+  const int big =
+      (int)(sizeof(float) * (9 * col_pitch(1 << QP_MAX_IND) + lt_floats(line_p(QP_MAX_IND))));
   for (int logn = 4; logn <= QP_MAX_IND; ++logn) {
     int rc = 0;
     QP_LINE_SWITCH(logn, rc = set_slice_smem<P_>(big));
