@@ -81,6 +81,41 @@ struct DevStatus {
 
 enum { QP_OK = 0, QP_OVERFLOW = 1 };
 
+// Programmatic dependent launch.  The slice kernels are launched with
+// launch_pdl, which lets a grid's CTAs start on the SMs that the grid before
+// it in the stream no longer fills.  Every kernel therefore opens with
+// grid_dep_sync() before it touches device data: griddepcontrol.wait returns
+// once the preceding grid has completed and its writes are visible (at once
+// for a kernel launched without the attribute), and launch_dependents then
+// allows the next grid to be scheduled behind this one.  Data that no kernel
+// writes (the twiddle tables) may be read before the wait.
+__device__ __forceinline__ void grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_sync() {
+  grid_dep_wait();
+  grid_dep_launch();
+}
+
+template <typename... KP, typename... A>
+inline cudaError_t launch_pdl(void (*k)(KP...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, A... a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, a...);
+}
+
 }  // namespace qp
 
 #define QP_CUDA_CHECK(call)                                                         \

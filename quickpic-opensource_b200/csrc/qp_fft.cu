@@ -129,6 +129,9 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
   const int n = g.nx, pitch = line_pitch(n);
   float* L = smem + warp * pitch;
   float* S = smem + (8 + warp) * pitch;
+  float* T = smem + line_count(g.indx) * pitch;
+  if (P > 0) stage_lane_table(T, tx);  // constant tables: staged before the wait
+  grid_dep_sync();
   if (st && st->error) return;
   const XComp c = job.c[blockIdx.y];
   const int y0 = blockIdx.x * 8;
@@ -138,11 +141,7 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
     if (!cursor_ok(c, st)) return;
     cur = (long long)st->cursor * c.cursor_stride;
   }
-  float* T = smem + line_count(g.indx) * pitch;
-  if (P > 0) {
-    stage_lane_table(T, tx);
-    __syncthreads();
-  }
+  if (P > 0) __syncthreads();
   if (y <= g.ny) {
     const float* s1 = c.src + cur + (long long)y * g.rp;
     const float* s2 = c.src2 ? c.src2 + (long long)y * g.rp : nullptr;
@@ -165,12 +164,14 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   extern __shared__ __align__(16) float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = g.nx, pitch = line_pitch(n);
+  float* T = smem + line_count(g.indx) * pitch;
+  // constant tables, staged before the wait; the barrier after the gather covers them
+  if (P > 0) stage_lane_table(T, tx);
+  grid_dep_sync();
   if (st && st->error) return;
   const XComp c = job.c[blockIdx.y];
   if (c.cursor_stride && !cursor_ok(c, st)) return;
   const int y0 = blockIdx.x * 8;
-  float* T = smem + line_count(g.indx) * pitch;
-  if (P > 0) stage_lane_table(T, tx);  // covered by the barrier after the gather
   for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
     const int r = idx & 7, kx = idx >> 3;
     const int yy = y0 + r;
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
 template <int P>
 __global__ void __launch_bounds__(256) k_ycol(YJob job, GridDims g, LineTables ty,
                                               const DevStatus* st) {
+  grid_dep_sync();
   extern __shared__ __align__(16) float smem[];
   if (st && st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -258,19 +260,19 @@ int fft_kernels_init() {
 void launch_xfwd(const XJob& job, const GridDims& g, const LineTables& tx, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.ny + 1 + 7) / 8, job.ncomp);
-  QP_LINE_SWITCH(g.indx, (k_xfwd<P_><<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st)));
+  QP_LINE_SWITCH(g.indx, (launch_pdl(k_xfwd<P_>, grid, 256, xpass_smem(g), s, job, g, tx, st)));
 }
 
 void launch_xinv(const XJob& job, const GridDims& g, const LineTables& tx, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.ny + 1 + 7) / 8, job.ncomp);
-  QP_LINE_SWITCH(g.indx, (k_xinv<P_><<<grid, 256, xpass_smem(g), s>>>(job, g, tx, st)));
+  QP_LINE_SWITCH(g.indx, (launch_pdl(k_xinv<P_>, grid, 256, xpass_smem(g), s, job, g, tx, st)));
 }
 
 void launch_ycol(const YJob& job, const GridDims& g, const LineTables& ty, const DevStatus* st,
                  cudaStream_t s) {
   dim3 grid((g.nx + 1 + 7) / 8);
-  QP_LINE_SWITCH(g.indy, (k_ycol<P_><<<grid, 256, ypass_smem(g), s>>>(job, g, ty, st)));
+  QP_LINE_SWITCH(g.indy, (launch_pdl(k_ycol<P_>, grid, 256, ypass_smem(g), s, job, g, ty, st)));
 }
 
 }  // namespace qp

@@ -16,6 +16,7 @@ __device__ __forceinline__ bool kidx(const GridDims& g, int i, int* kx, int* ky)
 
 __global__ void k_kpoint(int op, GridDims g, KCoef K, KPtrs in, KPtrs out, float aa, float dex,
                          const DevStatus* st) {
+  grid_dep_sync();
   if (st && st->error) return;
   int kx, ky;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -70,6 +71,7 @@ __global__ void k_kpoint(int op, GridDims g, KCoef K, KPtrs in, KPtrs out, float
 
 __global__ void k_lin(long long n, float* d, const float* a, const float* b, float v, int op,
                       const DevStatus* st) {
+  grid_dep_sync();
   if (st && st->error) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -95,6 +97,7 @@ __global__ void k_lin(long long n, float* d, const float* a, const float* b, flo
 
 // copyguard: row ny = row 0, every column (ufield2d_lib.f03:37-42)
 __global__ void k_guard_copy(float* p, GridDims g, const DevStatus* st) {
+  grid_dep_sync();
   if (st && st->error) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j <= g.nx + 1) p[(long long)g.ny * g.rp + j] = p[j];
@@ -102,6 +105,7 @@ __global__ void k_guard_copy(float* p, GridDims g, const DevStatus* st) {
 
 // acopyguard: row 0 += row ny, row ny = 0 for columns 0..nx (ufield2d_lib.f03:90-97)
 __global__ void k_guard_add(float* p, GridDims g, const DevStatus* st) {
+  grid_dep_sync();
   if (st && st->error) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j <= g.nx) {
@@ -116,6 +120,7 @@ __global__ void k_guard_add(float* p, GridDims g, const DevStatus* st) {
 __global__ void k_assemble(GridDims g, float* bx, float* by, float* bz, const float* ex,
                            const float* ey, const float* ebx, const float* eby, float dex,
                            const DevStatus* st) {
+  grid_dep_sync();
   if (st->error) return;
   int kx, ky;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -132,6 +137,7 @@ __global__ void k_assemble(GridDims g, float* bx, float* by, float* bz, const fl
 // (simulation_class.f03:725-726): dcu = dcu*dxi; cu(1:2) = cu(1:2) - dcu(1:2)
 __global__ void k_extrap(GridDims g, float* cx, float* cy, float* dx, float* dy, float dxi,
                          const DevStatus* st) {
+  grid_dep_sync();
   if (st->error) return;
   int kx, ky;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,6 +152,7 @@ __global__ void k_extrap(GridDims g, float* cx, float* cy, float* dx, float* dy,
 
 // Fourier-space scale of one plane, skipped after an error
 __global__ void k_kscale(GridDims g, float* p, float v, const DevStatus* st) {
+  grid_dep_sync();
   if (st->error) return;
   int kx, ky;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -162,6 +169,7 @@ __global__ void k_kscale(GridDims g, float* p, float v, const DevStatus* st) {
 __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by, const float* bz,
                           const float* psit, Planes3 be, Planes3 bb, float dex, int store,
                           int nplanes, float* zero_q, DevStatus* st) {
+  grid_dep_sync();
   if (st->error) return;
   const int cur = st->cursor;
   if (store && (cur < 0 || cur >= nplanes)) {  // never store outside the 3D arrays
@@ -218,6 +226,7 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
 }
 
 __global__ void k_cursor(DevStatus* st, int v) {
+  grid_dep_sync();
   if (st->error) return;
   st->cursor = v < 0 ? st->cursor + 1 : v;
 }
@@ -232,7 +241,7 @@ int launch_kpoint(int op, const GridDims& g, const KCoef& K, float* const* in, f
     b.p[i] = out ? out[i] : nullptr;
   }
   const int n = (g.nx + 1) * (g.ny + 1);
-  k_kpoint<<<(n + 255) / 256, 256, 0, s>>>(op, g, K, a, b, aa, dex, st);
+  launch_pdl(k_kpoint, (n + 255) / 256, 256, 0, s, op, g, K, a, b, aa, dex, st);
   return 0;
 }
 
@@ -241,44 +250,46 @@ void launch_lin(long long n, float* d, const float* a, const float* b, float v, 
   long long blocks = (n + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
   if (blocks < 1) blocks = 1;
-  k_lin<<<(int)blocks, 256, 0, s>>>(n, d, a, b, v, op, st);
+  launch_pdl(k_lin, (int)blocks, 256, 0, s, n, d, a, b, v, op, st);
 }
 
 void launch_guard_copy(float* p, const GridDims& g, const DevStatus* st, cudaStream_t s) {
-  k_guard_copy<<<(g.nx + 2 + 255) / 256, 256, 0, s>>>(p, g, st);
+  launch_pdl(k_guard_copy, (g.nx + 2 + 255) / 256, 256, 0, s, p, g, st);
 }
 
 void launch_guard_add(float* p, const GridDims& g, const DevStatus* st, cudaStream_t s) {
-  k_guard_add<<<(g.nx + 1 + 255) / 256, 256, 0, s>>>(p, g, st);
+  launch_pdl(k_guard_add, (g.nx + 1 + 255) / 256, 256, 0, s, p, g, st);
 }
 
 void launch_assemble(const GridDims& g, float* const* bxyz, float* const* epw,
                      float* const* epwb, float dex, const DevStatus* st, cudaStream_t s) {
   const int n = (g.nx + 1) * (g.ny + 1);
-  k_assemble<<<(n + 255) / 256, 256, 0, s>>>(g, bxyz[0], bxyz[1], bxyz[2], epw[0], epw[1],
+  launch_pdl(k_assemble, (n + 255) / 256, 256, 0, s, g, bxyz[0], bxyz[1], bxyz[2], epw[0], epw[1],
                                              epwb[0], epwb[1], dex, st);
 }
 
 void launch_extrap(const GridDims& g, float* const* cu, float* const* dcu, float dxi,
                    const DevStatus* st, cudaStream_t s) {
   const int n = (g.nx + 1) * (g.ny + 1);
-  k_extrap<<<(n + 255) / 256, 256, 0, s>>>(g, cu[0], cu[1], dcu[0], dcu[1], dxi, st);
+  launch_pdl(k_extrap, (n + 255) / 256, 256, 0, s, g, cu[0], cu[1], dcu[0], dcu[1], dxi, st);
 }
 
 void launch_kscale(const GridDims& g, float* p, float v, const DevStatus* st, cudaStream_t s) {
   const int n = (g.nx + 1) * (g.ny + 1);
-  k_kscale<<<(n + 255) / 256, 256, 0, s>>>(g, p, v, st);
+  launch_pdl(k_kscale, (n + 255) / 256, 256, 0, s, g, p, v, st);
 }
 
-void launch_cursor(DevStatus* st, int v, cudaStream_t s) { k_cursor<<<1, 1, 0, s>>>(st, v); }
+void launch_cursor(DevStatus* st, int v, cudaStream_t s) {
+  launch_pdl(k_cursor, 1, 1, 0, s, st, v);
+}
 
 void launch_store3d(const GridDims& g, float* const* fxy, float* const* bxyz, const float* psit,
                     const Planes3& be, const Planes3& bb, float dex, int store, int nplanes,
                     float* zero_q, DevStatus* st, cudaStream_t s) {
   long long blocks = ((g.rplane >> 2) + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_store3d<<<(int)blocks, 256, 0, s>>>(g, fxy[0], fxy[1], bxyz[0], bxyz[1], bxyz[2], psit, be,
-                                        bb, dex, store, nplanes, zero_q, st);
+  launch_pdl(k_store3d, (int)blocks, 256, 0, s, g, fxy[0], fxy[1], bxyz[0], bxyz[1], bxyz[2],
+             psit, be, bb, dex, store, nplanes, zero_q, st);
 }
 
 }  // namespace qp

@@ -63,6 +63,7 @@ __device__ __forceinline__ void flush(const float* s, float* plane, const TileGe
 // registers before the shared-memory atomics.
 __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, float* q,
                                                      DevStatus* st) {
+  grid_dep_sync();
   __shared__ float sq[TN * TN];
   if (st && st->error) return;
   const int t = blockIdx.x;
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
 
 __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const float* psi,
                                                 float qbm, float dex, DevStatus* st) {
+  grid_dep_sync();
   __shared__ float sp[TN * TN];
   if (st && st->error) return;
   const int t = blockIdx.x;
@@ -270,6 +272,7 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
                                                float* dcy, float* amxx, float* amyy,
                                                float* amxy, float qbm, float dt, float dex,
                                                float scale, DevStatus* st) {
+  grid_dep_sync();
   __shared__ float sf[7][TN * TN];
   __shared__ float sa[8][TN * TN];
   if (st && st->error) return;
@@ -395,6 +398,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, TileGeom tg,
                                               GatherPlanes f, float qbm, float dt, float dex,
                                               DevStatus* st) {
+  grid_dep_sync();
   __shared__ float sf[6][TN * TN];
   __shared__ int wsum[8];
   __shared__ int sbase;
@@ -562,11 +566,12 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   if (MODE != 0 && threadIdx.x == 0) B.count[t] = sbase;
 }
 
-// Insert the movers of tile t after its stayers, sorted by their
-// (source tile, source slot) key so the particle order does not depend on the
-// order in which the atomics of the push handed out inbox slots.
+// Insert the movers of tile t after its stayers, sorted by their key so that
+// the particle order does not depend on the order in which the atomics of the
+// push handed out inbox slots.
 __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg, int p2max,
                                                 DevStatus* st) {
+  grid_dep_sync();
   extern __shared__ unsigned long long skey[];
   int* sidx = reinterpret_cast<int*>(skey + p2max);
   if (st && st->error) return;
@@ -647,36 +652,35 @@ void launch_insert(const PartBuf& B, const Inbox& ib, const TileGeom& tg, DevSta
   int p2 = 1;
   while (p2 < ib.cap) p2 <<= 1;
   const size_t smem = (size_t)p2 * (sizeof(unsigned long long) + sizeof(int));
-  k_insert<<<tg.ntiles, 256, smem, s>>>(B, ib, tg, p2, st);
+  launch_pdl(k_insert, tg.ntiles, 256, smem, s, B, ib, tg, p2, st);
 }
 
 void launch_deposit_rho(const PartBuf& P, const TileGeom& tg, float* q, const DevStatus* st,
                         cudaStream_t s) {
-  k_deposit_rho<<<tg.ntiles, 256, 0, s>>>(P, tg, q, const_cast<DevStatus*>(st));
+  launch_pdl(k_deposit_rho, tg.ntiles, 256, 0, s, P, tg, q, const_cast<DevStatus*>(st));
 }
 
 void launch_extpsi(const PartBuf& P, const TileGeom& tg, const float* psi, float qbm, float dex,
                    const DevStatus* st, cudaStream_t s) {
-  k_extpsi<<<tg.ntiles, 256, 0, s>>>(P, tg, psi, qbm, dex, const_cast<DevStatus*>(st));
+  launch_pdl(k_extpsi, tg.ntiles, 256, 0, s, P, tg, psi, qbm, dex, const_cast<DevStatus*>(st));
 }
 
 void launch_amjdp(const PartBuf& P, const TileGeom& tg, const GatherPlanes& f, float* const* acc,
                   float qbm, float dt, float dex, float scale, const DevStatus* st,
                   cudaStream_t s) {
-  k_amjdp<<<tg.ntiles, 256, 0, s>>>(P, tg, f, acc[0], acc[1], acc[2], acc[3], acc[4], acc[5],
-                                    acc[6], acc[7], qbm, dt, dex, scale,
-                                    const_cast<DevStatus*>(st));
+  launch_pdl(k_amjdp, tg.ntiles, 256, 0, s, P, tg, f, acc[0], acc[1], acc[2], acc[3], acc[4],
+             acc[5], acc[6], acc[7], qbm, dt, dex, scale, const_cast<DevStatus*>(st));
 }
 
 void launch_push(int mode, const PartBuf& A, const PartBuf& B, const Inbox& ib,
                  const TileGeom& tg, const GatherPlanes& f, float qbm, float dt, float dex,
                  DevStatus* st, cudaStream_t s) {
   if (mode == 0)
-    k_push<0><<<tg.ntiles, 256, 0, s>>>(A, B, ib, tg, f, qbm, dt, dex, st);
+    launch_pdl(k_push<0>, tg.ntiles, 256, 0, s, A, B, ib, tg, f, qbm, dt, dex, st);
   else if (mode == 1)
-    k_push<1><<<tg.ntiles, 256, 0, s>>>(A, B, ib, tg, f, qbm, dt, dex, st);
+    launch_pdl(k_push<1>, tg.ntiles, 256, 0, s, A, B, ib, tg, f, qbm, dt, dex, st);
   else
-    k_push<2><<<tg.ntiles, 256, 0, s>>>(A, B, ib, tg, f, qbm, dt, dex, st);
+    launch_pdl(k_push<2>, tg.ntiles, 256, 0, s, A, B, ib, tg, f, qbm, dt, dex, st);
 }
 
 }  // namespace qp

@@ -35,7 +35,6 @@ template <int P>
 __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, LineTables ty,
                                                  const DevStatus* st) {
   extern __shared__ __align__(16) float smem[];
-  if (st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = g.ny, pitch = col_pitch(n);
   const int kx = blockIdx.x;
@@ -46,10 +45,10 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   float* L = smem + warp * pitch;
   float* S = smem + (8 + warp) * pitch;
   float* T = smem + (P > 0 ? 8 : 16) * pitch;
-  if (P > 0) {
-    stage_lane_table(T, ty);
-    __syncthreads();
-  }
+  if (P > 0) stage_lane_table(T, ty);  // constant tables: staged before the wait
+  grid_dep_sync();
+  if (st->error) return;
+  if (P > 0) __syncthreads();
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
   if (warp == 0) {
     line_transform<P>(a.qe + co, nullptr, a.norm, L, S, g.indy, 0, ty, T, lane);
@@ -109,7 +108,6 @@ template <int P>
 __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, LineTables ty,
                                                  DevStatus* st) {
   extern __shared__ __align__(16) float smem[];
-  if (st->error) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = g.ny, pitch = col_pitch(n);
   const int kx = blockIdx.x;
@@ -120,10 +118,10 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
   float* L = smem + warp * pitch;
   float* S = smem + (9 + warp) * pitch;
   float* T = smem + (P > 0 ? 9 : 18) * pitch;
-  if (P > 0) {
-    stage_lane_table(T, ty);
-    __syncthreads();
-  }
+  if (P > 0) stage_lane_table(T, ty);  // constant tables: staged before the wait
+  grid_dep_sync();
+  if (st->error) return;
+  if (P > 0) __syncthreads();
   // phase 1: forward y of cu(3), dcu(2), amu(3): y parities S C S, S C, S S C
   if (warp < 8) {
     const int par = (warp == 1 || warp == 4 || warp == 7) ? 1 : 0;
@@ -222,12 +220,14 @@ int slice_kernels_init() {
 
 void launch_slice_a(const SliceA& a, const GridDims& g, const KCoef& K, const LineTables& ty,
                     const DevStatus* st, cudaStream_t s) {
-  QP_LINE_SWITCH(g.indy, (k_slice_a<P_><<<g.nx + 1, 256, slice_a_smem(g), s>>>(a, g, K, ty, st)));
+  QP_LINE_SWITCH(g.indy,
+                 (launch_pdl(k_slice_a<P_>, g.nx + 1, 256, slice_a_smem(g), s, a, g, K, ty, st)));
 }
 
 void launch_slice_b(const SliceB& b, const GridDims& g, const KCoef& K, const LineTables& ty,
                     DevStatus* st, cudaStream_t s) {
-  QP_LINE_SWITCH(g.indy, (k_slice_b<P_><<<g.nx + 1, 288, slice_b_smem(g), s>>>(b, g, K, ty, st)));
+  QP_LINE_SWITCH(g.indy,
+                 (launch_pdl(k_slice_b<P_>, g.nx + 1, 288, slice_b_smem(g), s, b, g, K, ty, st)));
 }
 
 }  // namespace qp
