@@ -391,17 +391,29 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   flush(sa[7], amxy, tg, noffp, moffp, scale);
 }
 
-// Push (mode 0, 1) and/or re-bin (mode 1, 2).  In modes 1 and 2 particles that
-// stay are compacted, in order, into B's tile; movers go to the destination
-// tile's inbox with a (source tile, source slot) key.
+// Push (mode 0, 1) and/or re-bin (mode 1, 2).  Mode 0 writes the pushed
+// particles back in place.  In modes 1 and 2 the particles that stay are
+// written to B's tile sorted by cell: the tile is taken in chunks of 1024
+// slots, the stayers of a chunk are held in shared memory and written out in
+// the order of a stable counting sort on their cell, so that the deposits see
+// runs of same-cell particles (k_deposit_rho, k_amjdp).  Movers go to the
+// destination tile's inbox with a (cell, source tile, source slot) key, which
+// the insert kernel sorts, so they too arrive in cell order.
+constexpr int PUSH_CHUNK = 1024;
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, TileGeom tg,
                                               GatherPlanes f, float qbm, float dt, float dex,
                                               DevStatus* st) {
   grid_dep_sync();
+  constexpr int CH = MODE != 0 ? PUSH_CHUNK : 1;
+  constexpr int NC = MODE != 0 ? 256 : 1;
   __shared__ float sf[6][TN * TN];
-  __shared__ int wsum[8];
-  __shared__ int sbase;
+  __shared__ float stg[NCOMP][CH];       // the chunk's stayers, by chunk slot
+  __shared__ short perm[CH];             // output order -> chunk slot
+  __shared__ unsigned char whist[8][NC];  // per warp: stayers of each cell in this round
+  __shared__ int cstart[NC];             // first output position of each cell
+  __shared__ int wtot[8];
   if (st && st->error) return;
   const int t = blockIdx.x;
   int noffp, moffp;
@@ -423,7 +435,8 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
       }
     }
   }
-  if (threadIdx.x == 0) sbase = 0;
+  if (MODE != 0)
+    for (int i = threadIdx.x; i < 8 * NC; i += blockDim.x) (&whist[0][0])[i] = 0;
   __syncthreads();
   const float idex = 1.f / dex;
   const float qtmh = 0.5f * qbm * dt;
@@ -437,12 +450,17 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   }
   const long long base = (long long)t * A.cap;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r0 = 0; r0 < n; r0 += blockDim.x) {
-    const int k = r0 + threadIdx.x;
-    const bool live = k < n;
-    float pc[NCOMP];
-    int dest = t;
-    if (live) {
+  const unsigned lt = (1u << lane) - 1u;
+  int written = 0;  // stayers written to B so far (the same in every thread)
+  for (int c0 = 0; c0 < n; c0 += (MODE != 0 ? CH : (int)blockDim.x)) {
+    int cellr[MODE != 0 ? CH / 256 : 1];
+#pragma unroll
+    for (int r = 0; r < (MODE != 0 ? CH / 256 : 1); ++r) {
+      const int slot = r * 256 + threadIdx.x;
+      const int k = c0 + slot;
+      cellr[r] = -1;
+      if (k >= n) continue;
+      float pc[NCOMP];
 #pragma unroll
       for (int c = 0; c < NCOMP; ++c) pc[c] = A.c[c][base + k];
       if (MODE != 2) {
@@ -504,66 +522,121 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
           if (dy + any >= any) pc[1] = 0.f;
         }
       }
-      if (MODE != 0) {
-        // re-insertion wrap of PPPORDER2LB (part2d_lib77.f:1936-1973)
-        float xw = pc[0], yw = pc[1];
-        if (xw < 0.f) xw = xw + anx;
-        if (xw >= anx) xw = xw - anx;
-        if (yw < 0.f) yw = yw + any;
-        if (yw >= any) yw = yw - any;
-        pc[0] = xw;
-        pc[1] = yw;
-        int tx = (int)xw / TILE, ty = (int)yw / TILE;
-        if (tx < 0 || tx >= tg.mx1 || ty < 0 || ty >= tg.myp1 || !(xw == xw) || !(yw == yw)) {
-          raise_error(st, -4);
-          tx = 0;
-          ty = 0;
-        }
-        dest = tx + tg.mx1 * ty;
-      } else {
+      if (MODE == 0) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) A.c[c][base + k] = pc[c];
+        continue;
       }
-    }
-    if (MODE != 0) {
-      const bool stay = live && dest == t;
-      const unsigned bal = __ballot_sync(0xffffffffu, stay);
-      if (lane == 0) wsum[warp] = __popc(bal);
-      __syncthreads();
-      int woff = 0;
-      for (int w = 0; w < warp; ++w) woff += wsum[w];
-      const int pos = sbase + woff + __popc(bal & ((1u << lane) - 1u));
-      if (stay) {
-        if (pos < B.cap) {
-          const long long o = (long long)t * B.cap + pos;
+      // re-insertion wrap of PPPORDER2LB (part2d_lib77.f:1936-1973)
+      float xw = pc[0], yw = pc[1];
+      if (xw < 0.f) xw = xw + anx;
+      if (xw >= anx) xw = xw - anx;
+      if (yw < 0.f) yw = yw + any;
+      if (yw >= any) yw = yw - any;
+      pc[0] = xw;
+      pc[1] = yw;
+      const int ix = (int)xw, iy = (int)yw;
+      int tx = ix / TILE, ty = iy / TILE;
+      if (tx < 0 || tx >= tg.mx1 || ty < 0 || ty >= tg.myp1 || !(xw == xw) || !(yw == yw)) {
+        raise_error(st, -4);
+        tx = 0;
+        ty = 0;
+      }
+      const int dest = tx + tg.mx1 * ty;
+      const int cell = (iy & (TILE - 1)) * TILE + (ix & (TILE - 1));
+      if (dest == t) {
+        cellr[r] = cell;
 #pragma unroll
-          for (int c = 0; c < NCOMP; ++c) B.c[c][o] = pc[c];
-        } else {
-          raise_error(st, QP_OVERFLOW);
-          atomicMax(&st->need_cap, pos + 1);
-        }
-      } else if (live) {
-        const int slot = atomicAdd(&ib.count[dest], 1);
-        if (slot < ib.cap) {
-          const long long o = (long long)dest * ib.cap + slot;
+        for (int c = 0; c < NCOMP; ++c) stg[c][slot] = pc[c];
+      } else {
+        const int islot = atomicAdd(&ib.count[dest], 1);
+        if (islot < ib.cap) {
+          const long long o = (long long)dest * ib.cap + islot;
 #pragma unroll
           for (int c = 0; c < NCOMP; ++c) ib.c[c][o] = pc[c];
-          ib.key[o] = ((unsigned long long)t << 32) | (unsigned)k;
+          ib.key[o] = ((unsigned long long)cell << 48) | ((unsigned long long)t << 24) |
+                      (unsigned long long)(k & 0xffffff);
         } else {
           raise_error(st, QP_OVERFLOW);
-          atomicMax(&st->need_inbox, slot + 1);
+          atomicMax(&st->need_inbox, islot + 1);
         }
       }
+    }
+    if (MODE == 0) continue;
+    // stayers per cell: one shared atomic per group of equal cells in a warp
+    cstart[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < CH / 256; ++r) {
+      const int cl = cellr[r];
+      const unsigned same = __match_any_sync(0xffffffffu, cl >= 0 ? cl : 256 + lane);
+      if (cl >= 0 && lane == __ffs(same) - 1) atomicAdd(&cstart[cl], __popc(same));
+    }
+    __syncthreads();
+    // exclusive scan over the 256 cells (thread c owns cell c); nst = the chunk's stayers
+    int nst;
+    {
+      const int v = cstart[threadIdx.x];
+      int inc = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+      }
+      if (lane == 31) wtot[warp] = inc;
       __syncthreads();
-      if (threadIdx.x == 0) {
-        int tot = 0;
-        for (int w = 0; w < 8; ++w) tot += wsum[w];
-        sbase += tot;
+      int off = 0;
+      nst = 0;
+      for (int w = 0; w < 8; ++w) {
+        if (w < warp) off += wtot[w];
+        nst += wtot[w];
+      }
+      cstart[threadIdx.x] = off + inc - v;
+    }
+    __syncthreads();
+    // stable ranks in slot order: round r holds slots r*256 .. r*256+255; within
+    // a round, equal cells are ranked by warp, then by lane
+#pragma unroll
+    for (int r = 0; r < CH / 256; ++r) {
+      const int cl = cellr[r];
+      const unsigned same = __match_any_sync(0xffffffffu, cl >= 0 ? cl : 256 + lane);
+      const bool lead = cl >= 0 && lane == __ffs(same) - 1;
+      if (lead) whist[warp][cl] = (unsigned char)__popc(same);
+      __syncthreads();
+      if (cl >= 0) {
+        int pos = cstart[cl] + __popc(same & lt);
+        for (int w = 0; w < warp; ++w) pos += whist[w][cl];
+        if (pos >= 0 && pos < CH)
+          perm[pos] = (short)(r * 256 + threadIdx.x);
+        else
+          raise_error(st, -8);
+      }
+      __syncthreads();
+      if (lead) {
+        atomicAdd(&cstart[cl], __popc(same));
+        whist[warp][cl] = 0;
       }
       __syncthreads();
     }
+    // write the chunk's stayers in cell order
+    for (int j = threadIdx.x; j < nst; j += blockDim.x) {
+      const int slot = perm[j];
+      const int pos = written + j;
+      if (slot < 0 || slot >= CH) {
+        raise_error(st, -8);
+      } else if (pos < B.cap) {
+        const long long o = (long long)t * B.cap + pos;
+#pragma unroll
+        for (int c = 0; c < NCOMP; ++c) B.c[c][o] = stg[c][slot];
+      } else {
+        raise_error(st, QP_OVERFLOW);
+        atomicMax(&st->need_cap, pos + 1);
+      }
+    }
+    written += nst;
+    __syncthreads();
   }
-  if (MODE != 0 && threadIdx.x == 0) B.count[t] = sbase;
+  if (MODE != 0 && threadIdx.x == 0) B.count[t] = written;
 }
 
 // Insert the movers of tile t after its stayers, sorted by their key so that

@@ -20,7 +20,7 @@ struct PartBuf {
 // the insert kernel).
 struct Inbox {
   float* c[NCOMP];
-  unsigned long long* key;  // (source tile << 32 | source slot): deterministic order
+  unsigned long long* key;  // cell << 48 | source tile << 24 | source slot: deterministic order
   int* count;     // per destination tile
   int cap;        // slots per tile
 };
