@@ -282,6 +282,58 @@ def run_fft_case(args, cfg):
     ctx.close()
 
 
+def run_amjdp_case(args, cfg):
+    """Kernel case: class-level amjdp (the current and acceleration deposit with the
+    half push, PPGRDCJPPOST2L_QP) of a 2 x 2 ppc plasma on the workload's transverse
+    grid.  The particles are moved by up to 2 cells, given thermal momenta and
+    re-binned (which leaves each tile in cell order, as in the step); the fields
+    are seeded random values.  One step = one call; the kernel can be profiled
+    without the rest of the slice."""
+    import qpgpu
+
+    g = cfg["grid"]
+    ctx = qpgpu.Context(g["ind"][0], g["ind"][1], 1, g["box"])
+    sp = qpgpu.Species2d(ctx, ppc=(2, 2), xtras=0.5)
+    pp, kp = sp.get_particles()
+    rng = np.random.default_rng(3)
+    for t in range(len(kp)):
+        n = kp[t]
+        pp[0, :n, t] += rng.uniform(-2.0, 2.0, n).astype(np.float32)
+        pp[1, :n, t] += rng.uniform(-2.0, 2.0, n).astype(np.float32)
+        for c in (2, 3, 4):
+            pp[c, :n, t] = rng.normal(0.0, 0.1, n).astype(np.float32)
+        for c in (5, 6):
+            pp[c, :n, t] = (1.0 + 0.01 * rng.standard_normal(n)).astype(np.float32)
+    np.clip(pp[0], 0.0, ctx.nx - 1e-3, out=pp[0])
+    np.clip(pp[1], 0.0, ctx.ny - 1e-3, out=pp[1])
+    sp.set_particles(pp, kp)
+    sp.pmove()
+    fxy, bxyz, psit = qpgpu.Field2d(ctx, 2), qpgpu.Field2d(ctx, 3), qpgpu.Field2d(ctx, 1)
+    cu, amu, dcu = qpgpu.Field2d(ctx, 3), qpgpu.Field2d(ctx, 3), qpgpu.Field2d(ctx, 2)
+    for f, d in ((fxy, 2), (bxyz, 3), (psit, 1)):
+        f.set_rs((0.01 * rng.standard_normal(ctx.rs_shape(d))).astype(np.float32))
+    dex = ctx.dex
+    for _ in range(args.warmup):
+        sp.amjdp(fxy, bxyz, psit, cu, amu, dcu, dex)
+    ctx.sync()
+    import torch
+
+    torch.cuda.profiler.start()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        sp.amjdp(fxy, bxyz, psit, cu, amu, dcu, dex)
+    ms = ctx.timer_stop()
+    torch.cuda.profiler.stop()
+    npart = sp.np()
+    print(json.dumps({"case": "amjdp", "grid": [ctx.nx, ctx.ny], "particles": npart,
+                      "steps": args.steps, "us_per_call": 1e3 * ms / args.steps,
+                      "particles_per_s": npart * args.steps / (ms * 1e-3)}), flush=True)
+    for f in (fxy, bxyz, psit, cu, amu, dcu):
+        f.close()
+    sp.close()
+    ctx.close()
+
+
 def _reduce(v, dist, op):
     if dist is None:
         return v
@@ -383,12 +435,16 @@ def main():
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="step", choices=["step", "fft"],
-                    help="step: the 3D step (the benchmark); fft: transform kernels alone")
+    ap.add_argument("--case", default="step", choices=["step", "fft", "amjdp"],
+                    help="step: the 3D step (the benchmark); fft: transform kernels alone; "
+                    "amjdp: the current deposit alone")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.case == "fft":
         run_fft_case(args, cfg)
+        return
+    if args.case == "amjdp":
+        run_amjdp_case(args, cfg)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
