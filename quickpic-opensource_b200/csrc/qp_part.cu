@@ -260,13 +260,33 @@ __device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, 
   o->v[7] = v3;
 }
 
+// Add a run's 8 x 4 corner sums (times scale) to the global planes: fire-and-
+// forget reductions in L2 (red.global.add.f32), native for FP32, where a
+// shared-memory float atomic is a compare-and-swap loop.  The top edge of the
+// top tile row folds onto row 0 (the single-rank guard add, PPNACGUARD2L).
+__device__ __forceinline__ void deposit_run(float* const* pl, const TileGeom& tg, int noffp,
+                                            int moffp, int cell, const float (*acc)[4],
+                                            float scale) {
+  const int nn = cell % TN, mm = cell / TN;
+  const long long o0 = (long long)(moffp + mm) * tg.rp + noffp + nn;
+  const int y1 = moffp + mm + 1;
+  const long long o2 = (long long)(y1 == tg.ny ? 0 : y1) * tg.rp + noffp + nn;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    atomicAdd(pl[q] + o0, acc[q][0] * scale);
+    atomicAdd(pl[q] + o0 + 1, acc[q][1] * scale);
+    atomicAdd(pl[q] + o2, acc[q][2] * scale);
+    atomicAdd(pl[q] + o2 + 1, acc[q][3] * scale);
+  }
+}
+
 // Each thread takes 4 consecutive particles (float4 loads of each component)
 // and keeps the deposits of a run of particles in one cell in registers,
-// flushing them to the shared tile accumulators when the cell changes.  With
-// the particles of a tile stored cell by cell, this cuts the shared-memory
-// atomics about 4x and spreads a warp's atomics over different cells.
-// The per-particle products are those of the reference; only the order in
-// which a node's contributions are summed differs.
+// adding them to the global planes when the cell changes (deposit_run).  With
+// the particles of a tile stored cell by cell, runs are long and a warp's
+// reductions spread over neighbouring nodes.  The per-particle products are
+// those of the reference; only the order in which a node's contributions are
+// summed differs.  The planes must be zero on entry.
 __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, GatherPlanes f,
                                                float* cux, float* cuy, float* cuz, float* dcx,
                                                float* dcy, float* amxx, float* amyy,
@@ -274,8 +294,8 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
                                                float scale, DevStatus* st) {
   grid_dep_sync();
   __shared__ float sf[7][TN * TN];
-  __shared__ float sa[8][TN * TN];
   if (st && st->error) return;
+  float* const pl[8] = {cux, cuy, cuz, dcx, dcy, amxx, amyy, amxy};
   const int t = blockIdx.x;
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
@@ -287,7 +307,6 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   stage(sf[5], f.psit, tg, noffp, moffp);
   const bool ext = f.psi != nullptr;
   if (ext) stage(sf[6], f.psi, tg, noffp, moffp);
-  for (int i = threadIdx.x; i < 8 * TN * TN; i += blockDim.x) (&sa[0][0])[i] = 0.f;
   __syncthreads();
   const float qtmh = 0.5f * qbm * dt;
   const float dti = 1.f / dt;
@@ -344,15 +363,7 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
         p6o[j] = o.p6;
         const int c = mm * TN + nn;
         if (c != cell) {
-          if (cell >= 0) {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              atomicAdd(&sa[q][cell], acc[q][0]);
-              atomicAdd(&sa[q][cell + 1], acc[q][1]);
-              atomicAdd(&sa[q][cell + TN], acc[q][2]);
-              atomicAdd(&sa[q][cell + TN + 1], acc[q][3]);
-            }
-          }
+          if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc, scale);
           cell = c;
 #pragma unroll
           for (int q = 0; q < 8; ++q)
@@ -366,29 +377,12 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
         }
       }
     }
-    if (cell >= 0) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        atomicAdd(&sa[q][cell], acc[q][0]);
-        atomicAdd(&sa[q][cell + 1], acc[q][1]);
-        atomicAdd(&sa[q][cell + TN], acc[q][2]);
-        atomicAdd(&sa[q][cell + TN + 1], acc[q][3]);
-      }
-    }
+    if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc, scale);
     P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
     *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
     if (ext)
       *reinterpret_cast<float4*>(P.c[6] + base + k0) = make_float4(p7s[0], p7s[1], p7s[2], p7s[3]);
   }
-  __syncthreads();
-  flush(sa[0], cux, tg, noffp, moffp, scale);
-  flush(sa[1], cuy, tg, noffp, moffp, scale);
-  flush(sa[2], cuz, tg, noffp, moffp, scale);
-  flush(sa[3], dcx, tg, noffp, moffp, scale);
-  flush(sa[4], dcy, tg, noffp, moffp, scale);
-  flush(sa[5], amxx, tg, noffp, moffp, scale);
-  flush(sa[6], amyy, tg, noffp, moffp, scale);
-  flush(sa[7], amxy, tg, noffp, moffp, scale);
 }
 
 // Push (mode 0, 1) and/or re-bin (mode 1, 2).  Mode 0 writes the pushed
