@@ -1,11 +1,12 @@
 // qp_part.cu -- plasma particle kernels on tile-binned structure-of-arrays.
 //
-// One CTA owns one 16 x 16 cell tile (the reference's tile, part2d_class.f03:99):
-// it stages the 17 x 17 field nodes it interpolates from in shared memory,
-// accumulates deposits in shared memory, and flushes them to the global
-// planes once: nodes strictly inside the tile are written with plain stores
-// (no other tile touches them), shared edge nodes with atomics, and the top
-// edge of the top tile row is folded onto row 0 in the same flush -- the
+// One CTA owns one 16 x 16 cell tile (the reference's tile, part2d_class.f03:99)
+// and stages the 17 x 17 field nodes it interpolates from in shared memory.
+// The particles of a tile are kept in cell order (k_push), so the deposits sum
+// runs of same-cell particles in registers and add each run's corner sums to
+// the zeroed global planes with L2 reductions (red.global.add.f32, native for
+// FP32, where shared-memory float atomics are compare-and-swap loops).  The
+// top edge of the top tile row is folded onto row 0 as it is added -- the
 // single-rank guard add PPNACGUARD2L (ufield2d_lib.f03:90-97) done in-kernel.
 // Per-particle arithmetic follows the reference routines line by line:
 //   deposit_rho  PPGPPOST2L         part2d_lib77.f:194-309
@@ -14,8 +15,8 @@
 //   push         PPGRBPPUSHF23L_QP  part2d_lib77.f:1066-1408
 //   re-binning   PPPORDERF2LA/PPPORDER2LB part2d_lib77.f:1659-2028 (periodic
 //                wrap at re-insertion, part2d_lib77.f:1936-1973)
-// Every particle's cell is checked against its tile before shared memory is
-// indexed; a particle outside its tile raises a status error instead.
+// Every particle's cell is checked against its tile before it indexes shared
+// memory or a plane; a particle outside its tile raises a status error instead.
 #include "qp_part.cuh"
 
 namespace qp {
@@ -41,36 +42,30 @@ __device__ __forceinline__ void stage(float* s, const float* plane, const TileGe
   }
 }
 
-// flush a tile accumulator to a zeroed global plane (see file comment)
-__device__ __forceinline__ void flush(const float* s, float* plane, const TileGeom& tg, int noffp,
-                                      int moffp, float scale) {
-  for (int i = threadIdx.x; i < TN * TN; i += blockDim.x) {
-    const int a = i % TN, b = i / TN;
-    int gy = moffp + b;
-    const int gx = noffp + a;
-    if (gy == tg.ny) gy = 0;
-    const float v = s[i] * scale;
-    float* dst = plane + (long long)gy * tg.rp + gx;
-    if (a > 0 && a < TILE && b > 0 && b < TILE)
-      *dst = v;
-    else
-      atomicAdd(dst, v);
-  }
+// Add a run's 4 corner charges to the global plane q with L2 reductions
+// (red.global.add.f32), folding the top edge of the top tile row onto row 0.
+__device__ __forceinline__ void deposit_q(float* q, const TileGeom& tg, int noffp, int moffp,
+                                          int cell, const float* acc) {
+  const int nn = cell % TN, mm = cell / TN;
+  const long long o0 = (long long)(moffp + mm) * tg.rp + noffp + nn;
+  const int y1 = moffp + mm + 1;
+  const long long o2 = (long long)(y1 == tg.ny ? 0 : y1) * tg.rp + noffp + nn;
+  atomicAdd(q + o0, acc[0]);
+  atomicAdd(q + o0 + 1, acc[1]);
+  atomicAdd(q + o2, acc[2]);
+  atomicAdd(q + o2 + 1, acc[3]);
 }
 
 // Charge deposit with the run scheme of k_amjdp: 4 consecutive particles per
 // thread, corner weights of a run of particles in one cell summed in
-// registers before the shared-memory atomics.
+// registers, then added to q (which must be zero on entry) by deposit_q.
 __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, float* q,
                                                      DevStatus* st) {
   grid_dep_sync();
-  __shared__ float sq[TN * TN];
   if (st && st->error) return;
   const int t = blockIdx.x;
-  for (int i = threadIdx.x; i < TN * TN; i += blockDim.x) sq[i] = 0.f;
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
-  __syncthreads();
   const int n = P.count[t];
   if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
     if (threadIdx.x == 0) raise_error(st, -6);
@@ -102,12 +97,7 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
         const float w0 = amx * amy, w1 = dxp * amy, w2 = amx * dyp, w3 = dxp * dyp;
         const int c = mm * TN + nn;
         if (c != cell) {
-          if (cell >= 0) {
-            atomicAdd(sq + cell, acc[0]);
-            atomicAdd(sq + cell + 1, acc[1]);
-            atomicAdd(sq + cell + TN, acc[2]);
-            atomicAdd(sq + cell + TN + 1, acc[3]);
-          }
+          if (cell >= 0) deposit_q(q, tg, noffp, moffp, cell, acc);
           cell = c;
           acc[0] = w0;
           acc[1] = w1;
@@ -121,15 +111,8 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
         }
       }
     }
-    if (cell >= 0) {
-      atomicAdd(sq + cell, acc[0]);
-      atomicAdd(sq + cell + 1, acc[1]);
-      atomicAdd(sq + cell + TN, acc[2]);
-      atomicAdd(sq + cell + TN + 1, acc[3]);
-    }
+    if (cell >= 0) deposit_q(q, tg, noffp, moffp, cell, acc);
   }
-  __syncthreads();
-  flush(sq, q, tg, noffp, moffp, 1.f);
 }
 
 __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const float* psi,
