@@ -282,13 +282,15 @@ def run_fft_case(args, cfg):
     ctx.close()
 
 
-def run_amjdp_case(args, cfg):
-    """Kernel case: class-level amjdp (the current and acceleration deposit with the
-    half push, PPGRDCJPPOST2L_QP) of a 2 x 2 ppc plasma on the workload's transverse
-    grid.  The particles are moved by up to 2 cells, given thermal momenta and
-    re-binned (which leaves each tile in cell order, as in the step); the fields
-    are seeded random values.  One step = one call; the kernel can be profiled
-    without the rest of the slice."""
+def run_particle_case(args, cfg):
+    """Kernel cases: one class-level particle routine of a 2 x 2 ppc plasma on the
+    workload's transverse grid -- amjdp (the current and acceleration deposit
+    with the half push, PPGRDCJPPOST2L_QP) or push (the full push with the
+    re-bin, PPGRBPPUSHF23L_QP + PPPORDERF2LA/PPPORDER2LB).  The particles are
+    moved by up to 2 cells, given thermal momenta and re-binned (which leaves
+    each tile in cell order, as in the step); the fields are seeded random
+    values.  One step = one call; the kernel can be profiled without the rest
+    of the slice."""
     import qpgpu
 
     g = cfg["grid"]
@@ -313,19 +315,25 @@ def run_amjdp_case(args, cfg):
     for f, d in ((fxy, 2), (bxyz, 3), (psit, 1)):
         f.set_rs((0.01 * rng.standard_normal(ctx.rs_shape(d))).astype(np.float32))
     dex = ctx.dex
+    if args.case == "amjdp":
+        def call():
+            sp.amjdp(fxy, bxyz, psit, cu, amu, dcu, dex)
+    else:
+        def call():
+            sp.push(fxy, bxyz, psit, dex)
     for _ in range(args.warmup):
-        sp.amjdp(fxy, bxyz, psit, cu, amu, dcu, dex)
+        call()
     ctx.sync()
     import torch
 
     torch.cuda.profiler.start()
     ctx.timer_start()
     for _ in range(args.steps):
-        sp.amjdp(fxy, bxyz, psit, cu, amu, dcu, dex)
+        call()
     ms = ctx.timer_stop()
     torch.cuda.profiler.stop()
     npart = sp.np()
-    print(json.dumps({"case": "amjdp", "grid": [ctx.nx, ctx.ny], "particles": npart,
+    print(json.dumps({"case": args.case, "grid": [ctx.nx, ctx.ny], "particles": npart,
                       "steps": args.steps, "us_per_call": 1e3 * ms / args.steps,
                       "particles_per_s": npart * args.steps / (ms * 1e-3)}), flush=True)
     for f in (fxy, bxyz, psit, cu, amu, dcu):
@@ -435,16 +443,16 @@ def main():
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="step", choices=["step", "fft", "amjdp"],
+    ap.add_argument("--case", default="step", choices=["step", "fft", "amjdp", "push"],
                     help="step: the 3D step (the benchmark); fft: transform kernels alone; "
-                    "amjdp: the current deposit alone")
+                    "amjdp / push: one particle routine alone")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.case == "fft":
         run_fft_case(args, cfg)
         return
-    if args.case == "amjdp":
-        run_amjdp_case(args, cfg)
+    if args.case in ("amjdp", "push"):
+        run_particle_case(args, cfg)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
