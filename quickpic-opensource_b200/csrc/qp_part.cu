@@ -373,7 +373,10 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
 // written to B's tile sorted by cell: the tile is taken in chunks of 1024
 // slots, the stayers of a chunk are held in shared memory and written out in
 // the order of a stable counting sort on their cell, so that the deposits see
-// runs of same-cell particles (k_deposit_rho, k_amjdp).  Movers go to the
+// runs of same-cell particles (k_deposit_rho, k_amjdp).  Warp w takes the
+// slots w * 128 .. w * 128 + 127 of a chunk, 32 per round, so a particle's
+// rank among the earlier same-cell stayers needs only its own warp's running
+// counts, and the chunk needs four CTA barriers.  Movers go to the
 // destination tile's inbox with a (cell, source tile, source slot) key, which
 // the insert kernel sorts, so they too arrive in cell order.
 constexpr int PUSH_CHUNK = 1024;
@@ -385,11 +388,12 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   grid_dep_sync();
   constexpr int CH = MODE != 0 ? PUSH_CHUNK : 1;
   constexpr int NC = MODE != 0 ? 256 : 1;
+  constexpr int NR = MODE != 0 ? CH / 256 : 1;  // rounds of 256 slots per chunk
   __shared__ float sf[6][TN * TN];
-  __shared__ float stg[NCOMP][CH];       // the chunk's stayers, by chunk slot
-  __shared__ short perm[CH];             // output order -> chunk slot
-  __shared__ unsigned char whist[8][NC];  // per warp: stayers of each cell in this round
-  __shared__ int cstart[NC];             // first output position of each cell
+  __shared__ float stg[NCOMP][CH];      // the chunk's stayers, by chunk slot
+  __shared__ short perm[CH];            // output order -> chunk slot
+  __shared__ unsigned char wcnt[8][NC];  // per warp: its stayers of each cell so far
+  __shared__ short woff[8][NC];         // per warp: first output position of each cell
   __shared__ int wtot[8];
   if (st && st->error) return;
   const int t = blockIdx.x;
@@ -413,7 +417,7 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
     }
   }
   if (MODE != 0)
-    for (int i = threadIdx.x; i < 8 * NC; i += blockDim.x) (&whist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < 8 * NC; i += blockDim.x) (&wcnt[0][0])[i] = 0;
   __syncthreads();
   const float idex = 1.f / dex;
   const float qtmh = 0.5f * qbm * dt;
@@ -430,10 +434,10 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   const unsigned lt = (1u << lane) - 1u;
   int written = 0;  // stayers written to B so far (the same in every thread)
   for (int c0 = 0; c0 < n; c0 += (MODE != 0 ? CH : (int)blockDim.x)) {
-    int cellr[MODE != 0 ? CH / 256 : 1];
+    int cellr[NR];
 #pragma unroll
-    for (int r = 0; r < (MODE != 0 ? CH / 256 : 1); ++r) {
-      const int slot = r * 256 + threadIdx.x;
+    for (int r = 0; r < NR; ++r) {
+      const int slot = MODE != 0 ? warp * (CH / 8) + r * 32 + lane : threadIdx.x;
       const int k = c0 + slot;
       cellr[r] = -1;
       if (k >= n) continue;
@@ -539,79 +543,82 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
         }
       }
     }
-    if (MODE == 0) continue;
-    // stayers per cell: one shared atomic per group of equal cells in a warp
-    cstart[threadIdx.x] = 0;
-    __syncthreads();
+    if constexpr (MODE != 0) {
+      // rank of each stayer among the same-cell stayers of lower slots in its
+      // warp: the warp's running count of the cell plus the lower lanes of this
+      // round that share the cell (warp-local, so __syncwarp suffices)
+      int rank[NR];
 #pragma unroll
-    for (int r = 0; r < CH / 256; ++r) {
-      const int cl = cellr[r];
-      const unsigned same = __match_any_sync(0xffffffffu, cl >= 0 ? cl : 256 + lane);
-      if (cl >= 0 && lane == __ffs(same) - 1) atomicAdd(&cstart[cl], __popc(same));
-    }
-    __syncthreads();
-    // exclusive scan over the 256 cells (thread c owns cell c); nst = the chunk's stayers
-    int nst;
-    {
-      const int v = cstart[threadIdx.x];
-      int inc = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += u;
+      for (int r = 0; r < NR; ++r) {
+        const int cl = cellr[r];
+        const unsigned same = __match_any_sync(0xffffffffu, cl >= 0 ? cl : 256 + lane);
+        rank[r] = cl >= 0 ? wcnt[warp][cl] + __popc(same & lt) : 0;
+        __syncwarp();
+        if (cl >= 0 && lane == __ffs(same) - 1) wcnt[warp][cl] += (unsigned char)__popc(same);
+        __syncwarp();
       }
-      if (lane == 31) wtot[warp] = inc;
       __syncthreads();
-      int off = 0;
-      nst = 0;
-      for (int w = 0; w < 8; ++w) {
-        if (w < warp) off += wtot[w];
-        nst += wtot[w];
-      }
-      cstart[threadIdx.x] = off + inc - v;
-    }
-    __syncthreads();
-    // stable ranks in slot order: round r holds slots r*256 .. r*256+255; within
-    // a round, equal cells are ranked by warp, then by lane
+      // thread c: the chunk's stayers of cell c, an exclusive scan over the cells,
+      // and the first position of each warp's stayers of cell c
+      int nst;
+      {
+        const int c = threadIdx.x;
+        int v = 0;
 #pragma unroll
-    for (int r = 0; r < CH / 256; ++r) {
-      const int cl = cellr[r];
-      const unsigned same = __match_any_sync(0xffffffffu, cl >= 0 ? cl : 256 + lane);
-      const bool lead = cl >= 0 && lane == __ffs(same) - 1;
-      if (lead) whist[warp][cl] = (unsigned char)__popc(same);
+        for (int w = 0; w < 8; ++w) v += wcnt[w][c];
+        int inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int u = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += u;
+        }
+        if (lane == 31) wtot[warp] = inc;
+        __syncthreads();
+        int off = 0;
+        nst = 0;
+        for (int w = 0; w < 8; ++w) {
+          if (w < warp) off += wtot[w];
+          nst += wtot[w];
+        }
+        int pos = off + inc - v;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+          woff[w][c] = (short)pos;
+          pos += wcnt[w][c];
+          wcnt[w][c] = 0;  // ready for the next chunk (read again only after a barrier)
+        }
+      }
       __syncthreads();
-      if (cl >= 0) {
-        int pos = cstart[cl] + __popc(same & lt);
-        for (int w = 0; w < warp; ++w) pos += whist[w][cl];
-        if (pos >= 0 && pos < CH)
-          perm[pos] = (short)(r * 256 + threadIdx.x);
-        else
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const int cl = cellr[r];
+        if (cl >= 0) {
+          const int pos = woff[warp][cl] + rank[r];
+          if (pos >= 0 && pos < CH)
+            perm[pos] = (short)(warp * (CH / 8) + r * 32 + lane);
+          else
+            raise_error(st, -8);
+        }
+      }
+      __syncthreads();
+      // write the chunk's stayers in cell order
+      for (int j = threadIdx.x; j < nst; j += blockDim.x) {
+        const int slot = perm[j];
+        const int pos = written + j;
+        if (slot < 0 || slot >= CH) {
           raise_error(st, -8);
-      }
-      __syncthreads();
-      if (lead) {
-        atomicAdd(&cstart[cl], __popc(same));
-        whist[warp][cl] = 0;
-      }
-      __syncthreads();
-    }
-    // write the chunk's stayers in cell order
-    for (int j = threadIdx.x; j < nst; j += blockDim.x) {
-      const int slot = perm[j];
-      const int pos = written + j;
-      if (slot < 0 || slot >= CH) {
-        raise_error(st, -8);
-      } else if (pos < B.cap) {
-        const long long o = (long long)t * B.cap + pos;
+        } else if (pos < B.cap) {
+          const long long o = (long long)t * B.cap + pos;
 #pragma unroll
-        for (int c = 0; c < NCOMP; ++c) B.c[c][o] = stg[c][slot];
-      } else {
-        raise_error(st, QP_OVERFLOW);
-        atomicMax(&st->need_cap, pos + 1);
+          for (int c = 0; c < NCOMP; ++c) B.c[c][o] = stg[c][slot];
+        } else {
+          raise_error(st, QP_OVERFLOW);
+          atomicMax(&st->need_cap, pos + 1);
+        }
       }
+      written += nst;
+      __syncthreads();
     }
-    written += nst;
-    __syncthreads();
   }
   if (MODE != 0 && threadIdx.x == 0) B.count[t] = written;
 }
