@@ -237,6 +237,11 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * per-slice loop (643-736) as one fixed sequence of kernel launches per
  * slice, and the species renew.
  * iter = fixed number of B predictor-corrector passes (simulation.iter);
+ * tol = 0 runs exactly iter passes per slice, as the reference does; tol > 0
+ * stops a slice's passes after the first one whose relative change of the
+ * transverse B, |epw - epw_prev| / |epw| over all Fourier modes, is at most
+ * tol, and runs at most iter passes (one plasma species only; the passes
+ * actually run are returned in qp_step_stats.iterations);
  * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
  * use_graphs is accepted and ignored: the slices are launched directly;
  * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
@@ -247,7 +252,8 @@ typedef struct {
   int store3d;
   int use_graphs;
   float dt;
-  int reserved[4];
+  float tol;
+  int reserved[3];
 } qp_sim_desc;
 
 typedef struct {

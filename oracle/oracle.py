@@ -276,7 +276,7 @@ P_FIXED = 20
 B_NPAR = 18
 W = dict(psi=1, fxy=2, bxyz=3, psit=4, cu=5, dcu=6, amu=7, epw_k=8, cu_k=9, qe=10, qb=11,
          epwb_k=12, ppart=13, kpic=14, bexyz=15, bbxyz=16, q3=17, q3d=18, qn=19, beam0=20,
-         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25)
+         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26)
 
 
 def sim_params(cfg) -> np.ndarray:
@@ -296,6 +296,7 @@ def sim_params(cfg) -> np.ndarray:
     p[16] = len(cfg["beams"])
     p[17] = 1 if cfg.get("store3d", True) else 0
     p[18] = cfg.get("dt", 0.0)  # 3D time step; > 0 pushes the beams after the slices
+    p[19] = cfg.get("tol", 0.0)  # > 0: B passes per slice until |d epw| <= tol |epw|
     for b, bm in enumerate(cfg["beams"]):
         o = P_FIXED + B_NPAR * b
         p[o:o + 3] = bm["np"]

@@ -113,10 +113,11 @@ static int sync_status(qp_ctx* ctx, DevStatus* out) {
 
 static int clear_status(qp_ctx* ctx, int keep_cursor) {
   DevStatus s{};
-  if (keep_cursor) {
+  if (keep_cursor) {  // a recovery within a step: keep its cursor and pass count
     DevStatus cur;
     if (sync_status(ctx, &cur)) return -1;
     s.cursor = cur.cursor;
+    s.passes = cur.passes;
   }
   CK(cudaMemcpyAsync(ctx->st, &s, sizeof(DevStatus), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

@@ -72,12 +72,23 @@ struct DevStatus {
   int need_cap;       // particles a tile must hold
   int need_inbox;     // movers a tile must accept
   int cursor;         // slice cursor of the fused 3D step
-  int iter_done;      // iterations run in the current slice
+  int pass_done;      // convergence-controlled B loop: the pass of this slice
+                      // whose residual met the tolerance (0 = none yet)
   int store_ctas;     // CTA completion counter of the 3D store kernel
   int beam_drops;     // beam particles dropped at the conducting boundary
-  float resid_num;    // convergence residual accumulators
-  float resid_den;
+  float resid_num;    // residual of the current pass: sum |epw - epw_old|^2
+  float resid_den;    //                               sum |epw|^2
+  int pass_ctas;      // CTA completion counter of the residual decision
+  int passes;         // predictor-corrector passes run in this 3D step
 };
+
+// A kernel of pass `pass` (1-based; 0 = not part of a convergence-controlled
+// loop) has nothing to do once an earlier pass of the slice has converged.
+__device__ __forceinline__ bool pass_skipped(const DevStatus* st, int pass) {
+  if (pass <= 1) return false;
+  const int done = st->pass_done;
+  return done > 0 && done < pass;
+}
 
 enum { QP_OK = 0, QP_OVERFLOW = 1 };
 

@@ -133,6 +133,7 @@ __global__ void __launch_bounds__(256) k_xfwd(XJob job, GridDims g, LineTables t
   if (P > 0) stage_lane_table(T, tx);  // constant tables: staged before the wait
   grid_dep_sync();
   if (st && st->error) return;
+  if (pass_skipped(st, job.pass)) return;
   const XComp c = job.c[blockIdx.y];
   const int y0 = blockIdx.x * 8;
   const int y = y0 + warp;
@@ -169,6 +170,7 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   if (P > 0) stage_lane_table(T, tx);
   grid_dep_sync();
   if (st && st->error) return;
+  if (pass_skipped(st, job.pass)) return;
   const XComp c = job.c[blockIdx.y];
   if (c.cursor_stride && !cursor_ok(c, st)) return;
   const int y0 = blockIdx.x * 8;

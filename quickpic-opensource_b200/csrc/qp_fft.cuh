@@ -36,6 +36,7 @@ struct XJob {
   // cleared by the CTAs of component i % ncomp)
   float* zero[8];
   int nzero;
+  int pass;  // predictor-corrector pass of the launch (pass_skipped), 0 = none
 };
 
 struct YComp {

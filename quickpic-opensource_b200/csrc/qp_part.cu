@@ -278,6 +278,7 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   grid_dep_sync();
   __shared__ float sf[7][TN * TN];
   if (st && st->error) return;
+  if (pass_skipped(st, f.pass)) return;
   float* const pl[8] = {cux, cuy, cuz, dcx, dcy, amxx, amyy, amxy};
   const int t = blockIdx.x;
   int noffp, moffp;

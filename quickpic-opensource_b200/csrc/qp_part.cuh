@@ -40,6 +40,7 @@ struct GatherPlanes {
   const float* psit; // psit
   int combine;       // 1: the push uses -fxy + (by, -bx), the final slice force
   const float* psi;  // amjdp only, optional: form p6, p7 from psi first (extpsi)
+  int pass;          // amjdp only: predictor-corrector pass (pass_skipped), 0 = none
 };
 
 int part_kernels_init();

@@ -48,6 +48,8 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   if (P > 0) stage_lane_table(T, ty);  // constant tables: staged before the wait
   grid_dep_sync();
   if (st->error) return;
+  // a new slice: no pass of it has converged yet (the passes follow this kernel)
+  if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<DevStatus*>(st)->pass_done = 0;
   if (P > 0) __syncthreads();
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
   if (warp == 0) {
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
   if (P > 0) stage_lane_table(T, ty);  // constant tables: staged before the wait
   grid_dep_sync();
   if (st->error) return;
+  if (pass_skipped(st, b.pass)) return;
   if (P > 0) __syncthreads();
   // phase 1: forward y of cu(3), dcu(2), amu(3): y parities S C S, S C, S S C
   if (warp < 8) {
@@ -166,6 +169,21 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
     atomicAdd(&st->resid_den, r_den);
   }
   __syncthreads();
+  if (b.track_residual && threadIdx.x == 0) {
+    // the last CTA to finish has the complete sums: decide, and reset them for
+    // the next pass (which starts only after this kernel)
+    __threadfence();
+    if (atomicAdd(&st->pass_ctas, 1) == (int)gridDim.x - 1) {
+      __threadfence();
+      const float num = atomicAdd(&st->resid_num, 0.f), den = atomicAdd(&st->resid_den, 0.f);
+      if (num <= b.tol2 * den) st->pass_done = b.pass;
+      st->passes = st->passes + 1;
+      st->resid_num = 0.f;
+      st->resid_den = 0.f;
+      st->pass_ctas = 0;
+      __threadfence();
+    }
+  }
   // phase 3: inverse y of psit (S), bx (C), by (S), bz (C) and the smoothed q (S)
   if (warp < 4) {
     const int par = (warp == 1 || warp == 3) ? 1 : 0;

@@ -32,7 +32,12 @@ struct SliceB {
   float* q_out;
   float* zero[8];     // real-space planes to clear for the next pass
   int nzero;
+  // convergence-controlled loop: accumulate the relative change of B_perp,
+  // and let the last CTA mark the slice converged (DevStatus.pass_done = pass)
+  // when sum |epw - epw_old|^2 <= tol2 * sum |epw|^2
   int track_residual;
+  int pass;           // 1-based pass of this launch; later passes skip once converged
+  float tol2;
   float norm, dex, idex, aa, dxi;
 };
 

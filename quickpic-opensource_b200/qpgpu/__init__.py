@@ -96,7 +96,7 @@ class _BeamDesc(C.Structure):
 
 class _SimDesc(C.Structure):
     _fields_ = [("iter", C.c_int), ("store3d", C.c_int), ("use_graphs", C.c_int),
-                ("dt", C.c_float), ("reserved", C.c_int * 4)]
+                ("dt", C.c_float), ("tol", C.c_float), ("reserved", C.c_int * 3)]
 
 
 class StepStats(C.Structure):
@@ -407,9 +407,10 @@ class Simulation:
     """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
 
     def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False,
-                 dt=0.0):
+                 dt=0.0, tol=0.0):
         d = _SimDesc()
-        d.iter = iter
+        d.iter = iter  # passes per slice; with tol > 0 the most passes a slice may take
+        d.tol = tol  # > 0: stop a slice's passes once |d epw| / |epw| <= tol
         d.store3d = 1 if store3d else 0
         d.use_graphs = 1 if use_graphs else 0
         d.dt = dt  # 3D time step; > 0 ends every step with the beam push

@@ -338,7 +338,7 @@ def _gpu_sim(qp, cfg, use_graphs=False, dt=0.0):
                                peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
     sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs,
-                        dt=dt)
+                        dt=dt, tol=cfg.get("tol", 0.0))
     return c, sp, beams, sim
 
 
@@ -386,6 +386,34 @@ def test_full_3d_step_matches_oracle(qp, oracle_mod, use_graphs=False):
     for name in ("psit", "bxyz"):
         assert rel_l2(sim.get_field(name), o64.get(name).reshape(sim.get_field(name).shape,
                                                                  order="F")) < 1e-3, name
+    sim.close()
+    c.close()
+
+
+def test_convergence_controlled_step_matches_oracle(qp, oracle_mod):
+    """B passes stop per slice once |d epw| <= 1e-4 |epw| (at most 12), decided on
+    the device.  The pass count follows the FP64 oracle's (the FP32 residual may
+    cross the tolerance one pass earlier or later in a few slices) and the
+    converged fields match it."""
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 5), iter=12)
+    cfg["tol"] = 1e-4
+    c, sp, beams, sim = _gpu_sim(qp, cfg)
+    st = sim.step3d()
+    o64 = O.Sim(cfg, np.float64)
+    o64.begin3d()
+    for j in range(1, 33):
+        o64.slice(j)
+    passes = int(o64.get("passes")[0])
+    assert 2 * 32 < passes < 12 * 32
+    assert abs(st.iterations - passes) <= max(2, passes // 20), (st.iterations, passes)
+    be, bb = sim.get_3d("bexyz"), sim.get_3d("bbxyz")
+    assert rel_l2(be, o64.get("bexyz").reshape(be.shape, order="F")) < 1e-4
+    assert rel_l2(bb, o64.get("bbxyz").reshape(bb.shape, order="F")) < 1e-3
+    q3 = sim.get_3d("q3")
+    assert rel_l2(q3, o64.get("q3").reshape(q3.shape, order="F")) < 1e-4
+    # a second step starts the count again
+    assert sim.step3d().iterations > 2 * 32
     sim.close()
     c.close()
 

@@ -208,6 +208,39 @@ def test_fp32_oracle_tracks_fp64(oracle_mod):
     assert np.abs(s64.get("psi")).max() > 1e-3  # the beam drove a wake
 
 
+def _oracle_fields(O, cfg, nslices):
+    s = O.Sim(cfg, np.float64)
+    s.begin3d()
+    for j in range(1, nslices + 1):
+        s.slice(j)
+    out = s.get("bexyz").copy(), s.get("bbxyz").copy(), int(s.get("passes")[0])
+    s.close()
+    return out
+
+
+def test_convergence_control_approaches_many_passes(oracle_mod):
+    """With a tolerance, a slice's B passes stop once |d epw| <= tol |epw|.  The
+    converged fields lie closer to those of many fixed passes than the
+    reference's two passes do, and a tighter tolerance takes more passes."""
+    O = oracle_mod
+    ns = 12
+    cfg = make_config(ind=(5, 5, 4), iter=2)
+    e2, b2, _ = _oracle_fields(O, cfg, ns)
+    cfg = make_config(ind=(5, 5, 4), iter=16)
+    e16, b16, p16 = _oracle_fields(O, cfg, ns)
+    assert p16 == 0  # passes are counted only under a tolerance
+    res = {}
+    for tol in (1e-2, 1e-4):
+        cfg = make_config(ind=(5, 5, 4), iter=16)
+        cfg["tol"] = tol
+        res[tol] = _oracle_fields(O, cfg, ns)
+    ec, bc, pc = res[1e-4]
+    assert ns * 2 < pc < ns * 16
+    assert res[1e-2][2] < pc
+    assert rel_l2(bc, b16) < rel_l2(b2, b16)
+    assert rel_l2(ec, e16) < 1e-3
+
+
 def test_beam_push_free_streaming_and_drop(oracle_mod):
     """PGBPUSH32L_QP with zero fields: momenta unchanged, x += px dt/(dex gamma),
     z += (1 + p_perp^2) / (pz (pz + gamma)) dt/dxi; a particle that crosses
