@@ -262,6 +262,7 @@ typedef struct {
   int regrowths;       /* particle-buffer growths (overflow recoveries) */
   int kernels;         /* kernel launches of the step */
   double gpu_ms;       /* device time of the step */
+  int unconverged;     /* with tol > 0: slices whose iter-th pass still missed tol */
 } qp_step_stats;
 
 int qp_sim_create(qp_ctx* ctx, const qp_sim_desc* d, qp_species* const* species, int nspecies,

@@ -118,6 +118,7 @@ static int clear_status(qp_ctx* ctx, int keep_cursor) {
     if (sync_status(ctx, &cur)) return -1;
     s.cursor = cur.cursor;
     s.passes = cur.passes;
+    s.unconverged = cur.unconverged;
   }
   CK(cudaMemcpyAsync(ctx->st, &s, sizeof(DevStatus), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

@@ -80,6 +80,7 @@ struct DevStatus {
   float resid_den;    //                               sum |epw|^2
   int pass_ctas;      // CTA completion counter of the residual decision
   int passes;         // predictor-corrector passes run in this 3D step
+  int unconverged;    // slices of this step whose last allowed pass missed the tolerance
 };
 
 // A kernel of pass `pass` (1-based; 0 = not part of a convergence-controlled

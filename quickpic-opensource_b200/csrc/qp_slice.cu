@@ -176,7 +176,14 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
     if (atomicAdd(&st->pass_ctas, 1) == (int)gridDim.x - 1) {
       __threadfence();
       const float num = atomicAdd(&st->resid_num, 0.f), den = atomicAdd(&st->resid_den, 0.f);
-      if (num <= b.tol2 * den) st->pass_done = b.pass;
+      const int cur = st->cursor;
+      if (num <= b.tol2 * den) {
+        st->pass_done = b.pass;
+        if (b.slice_passes && cur >= 0 && cur <= b.max_slice) b.slice_passes[cur] = b.pass;
+      } else if (b.pass >= b.max_pass) {
+        st->unconverged = st->unconverged + 1;
+        if (b.slice_passes && cur >= 0 && cur <= b.max_slice) b.slice_passes[cur] = -b.pass;
+      }
       st->passes = st->passes + 1;
       st->resid_num = 0.f;
       st->resid_den = 0.f;

@@ -37,6 +37,9 @@ struct SliceB {
   // when sum |epw - epw_old|^2 <= tol2 * sum |epw|^2
   int track_residual;
   int pass;           // 1-based pass of this launch; later passes skip once converged
+  int max_pass;       // the last pass a slice may take
+  int* slice_passes;  // optional, per slice cursor: the converging pass, or -max_pass
+  int max_slice;      // last valid index of slice_passes
   float tol2;
   float norm, dex, idex, aa, dxi;
 };

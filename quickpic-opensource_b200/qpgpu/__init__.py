@@ -101,7 +101,7 @@ class _SimDesc(C.Structure):
 
 class StepStats(C.Structure):
     _fields_ = [("slices", C.c_int), ("iterations", C.c_int), ("regrowths", C.c_int),
-                ("kernels", C.c_int), ("gpu_ms", C.c_double)]
+                ("kernels", C.c_int), ("gpu_ms", C.c_double), ("unconverged", C.c_int)]
 
 
 class Context:

@@ -412,8 +412,13 @@ def test_convergence_controlled_step_matches_oracle(qp, oracle_mod):
     assert rel_l2(bb, o64.get("bbxyz").reshape(bb.shape, order="F")) < 1e-3
     q3 = sim.get_3d("q3")
     assert rel_l2(q3, o64.get("q3").reshape(q3.shape, order="F")) < 1e-4
-    # a second step starts the count again
-    assert sim.step3d().iterations > 2 * 32
+    # a second step of the same beam starts the count again, and enqueues each
+    # slice's passes from the first step's record (plus a margin): it runs the
+    # same passes and no slice runs out of them
+    st2 = sim.step3d()
+    assert abs(st2.iterations - st.iterations) <= 4, (st2.iterations, st.iterations)
+    assert st2.unconverged <= st.unconverged
+    assert st2.kernels < st.kernels
     sim.close()
     c.close()
 
