@@ -294,8 +294,10 @@ int qp_sim_download_lineout(qp_sim* sim, int comp, float* out);
  * the reference's per-step ELOG stamps, simulation_class.f03:614-645).
  * Kernel names are written newline-separated into `names`; ms[i], count[i] and
  * bytes[i] are the total milliseconds, launches and algorithmic bytes
- * (minimal FP32 traffic of the work done) of name i.  Returns the number of
- * names (<= max), or < 0 on error.  The species are renewed afterwards. */
+ * (minimal FP32 traffic of the work done) of name i.  Under a convergence
+ * tolerance the profiled slices run two fixed passes, so that every timed
+ * launch does its work.  Returns the number of names (<= max), or < 0 on
+ * error.  The species are renewed afterwards. */
 int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double* ms, int* count,
                    double* bytes, int max);
 

@@ -276,7 +276,7 @@ P_FIXED = 20
 B_NPAR = 18
 W = dict(psi=1, fxy=2, bxyz=3, psit=4, cu=5, dcu=6, amu=7, epw_k=8, cu_k=9, qe=10, qb=11,
          epwb_k=12, ppart=13, kpic=14, bexyz=15, bbxyz=16, q3=17, q3d=18, qn=19, beam0=20,
-         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26)
+         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26, unconverged=27)
 
 
 def sim_params(cfg) -> np.ndarray:

@@ -80,8 +80,20 @@ struct DevStatus {
   float resid_den;    //                               sum |epw|^2
   int pass_ctas;      // CTA completion counter of the residual decision
   int passes;         // predictor-corrector passes run in this 3D step
-  int unconverged;    // slices of this step whose last allowed pass missed the tolerance
+  int unconverged;    // slices of this step that stopped without meeting the tolerance
+  float resid_hist[2];  // this slice's squared relative residuals, one and two passes back
 };
+
+// Convergence control of the B passes of a slice (k_slice_b and the oracle):
+// with r the squared relative change of B_perp after pass `pass`, the slice
+// has converged once r <= tol^2; from pass QP_STALL_PASS on it has stalled
+// (the FP32 iteration can settle into a cycle above the tolerance) once r is
+// no longer below 0.81 times the smaller of the two previous values, i.e. the
+// relative change stopped dropping by 10 %.
+#define QP_STALL_PASS 8
+__host__ __device__ inline bool pass_stalled(int pass, float r, float r1, float r2) {
+  return pass >= QP_STALL_PASS && r >= 0.81f * fminf(r1, r2);
+}
 
 // A kernel of pass `pass` (1-based; 0 = not part of a convergence-controlled
 // loop) has nothing to do once an earlier pass of the slice has converged.

@@ -49,7 +49,11 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   grid_dep_sync();
   if (st->error) return;
   // a new slice: no pass of it has converged yet (the passes follow this kernel)
-  if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<DevStatus*>(st)->pass_done = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    DevStatus* ws = const_cast<DevStatus*>(st);
+    ws->pass_done = 0;
+    ws->resid_hist[0] = ws->resid_hist[1] = 1e30f;
+  }
   if (P > 0) __syncthreads();
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
   if (warp == 0) {
@@ -177,13 +181,18 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
       __threadfence();
       const float num = atomicAdd(&st->resid_num, 0.f), den = atomicAdd(&st->resid_den, 0.f);
       const int cur = st->cursor;
-      if (num <= b.tol2 * den) {
+      const float r = den > 0.f ? num / den : (num > 0.f ? 1.f : 0.f);
+      const bool stalled = pass_stalled(b.pass, r, st->resid_hist[0], st->resid_hist[1]);
+      if (r <= b.tol2) {
         st->pass_done = b.pass;
         if (b.slice_passes && cur >= 0 && cur <= b.max_slice) b.slice_passes[cur] = b.pass;
-      } else if (b.pass >= b.max_pass) {
+      } else if (stalled || b.pass >= b.max_pass) {
+        if (stalled) st->pass_done = b.pass;
         st->unconverged = st->unconverged + 1;
         if (b.slice_passes && cur >= 0 && cur <= b.max_slice) b.slice_passes[cur] = -b.pass;
       }
+      st->resid_hist[1] = st->resid_hist[0];
+      st->resid_hist[0] = r;
       st->passes = st->passes + 1;
       st->resid_num = 0.f;
       st->resid_den = 0.f;
