@@ -96,6 +96,7 @@ int qp_field2d_pot(qp_field2d* src, qp_field2d* dst);    /* MPPOTPD2 via field2d
 int qp_field2d_smooth(qp_field2d* src, qp_field2d* dst); /* MPPSMOOTHD2 via field2d%smooth 341-362 */
 int qp_field2d_elf(qp_field2d* src, qp_field2d* dst);    /* MPPOISD22 via field2d%elf 364-385 */
 int qp_field2d_bf(qp_field2d* src, qp_field2d* dst);     /* MPPBBPOISD23 via field2d%bf 387-408 */
+int qp_field2d_vpot(qp_field2d* src, qp_field2d* dst);   /* PBPOISD23 isign=1 via field2d%vpot 318-339 */
 int qp_field2d_div(qp_field2d* src, qp_field2d* dst);    /* MPPDIVFD2 via field2d%div 229-249 */
 int qp_field2d_grad(qp_field2d* src, qp_field2d* dst);   /* MPPGRADFD2 via field2d%grad 251-271 */
 /* field2d%bfqp (field2d_class.f03:410-432 -> PBPOISD22N_QP): the transverse-B
@@ -243,6 +244,9 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * tol, and runs at most iter passes (one plasma species only; the passes
  * actually run are returned in qp_step_stats.iterations);
  * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
+ * vpot = 1 (with store3d = 1, one species) also keeps the vector potential
+ * vpot3d of every slice (simulation_class.f03:711-716: field2d%vpot of the
+ * last pass's current, fftkr, times -dex), downloaded as "vpot";
  * use_graphs is accepted and ignored: the slices are launched directly;
  * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
  * step with beam3d%push of every beam with the stored bexyz, bbxyz
@@ -253,7 +257,8 @@ typedef struct {
   int use_graphs;
   float dt;
   float tol;
-  int reserved[3];
+  int vpot;
+  int reserved[2];
 } qp_sim_desc;
 
 typedef struct {

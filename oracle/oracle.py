@@ -130,6 +130,10 @@ def bf(cu, bxy, t, indx, indy):
     _call("oq_bf", cu.dtype, cu, bxy, t, indx, indy)
 
 
+def vpot(cu, a, t, indx, indy):
+    _call("oq_vpot", cu.dtype, cu, a, t, indx, indy)
+
+
 def bfqp(cu, dcu, amu, bxy, t, aa, dex, indx, indy):
     _call("oq_bfqp", cu.dtype, cu, dcu, amu, bxy, t, float(aa), float(dex), indx, indy)
 
@@ -272,11 +276,11 @@ def beam_push(part, fxyz, bxyz, qbm, dt, dex, dxi, ind3, dtype=np.float32):
 
 
 # -------------------------------------------------------------- simulation
-P_FIXED = 20
+P_FIXED = 21
 B_NPAR = 18
 W = dict(psi=1, fxy=2, bxyz=3, psit=4, cu=5, dcu=6, amu=7, epw_k=8, cu_k=9, qe=10, qb=11,
          epwb_k=12, ppart=13, kpic=14, bexyz=15, bbxyz=16, q3=17, q3d=18, qn=19, beam0=20,
-         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26, unconverged=27)
+         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26, unconverged=27, vpot3d=28)
 
 
 def sim_params(cfg) -> np.ndarray:
@@ -297,6 +301,7 @@ def sim_params(cfg) -> np.ndarray:
     p[17] = 1 if cfg.get("store3d", True) else 0
     p[18] = cfg.get("dt", 0.0)  # 3D time step; > 0 pushes the beams after the slices
     p[19] = cfg.get("tol", 0.0)  # > 0: B passes per slice until |d epw| <= tol |epw|
+    p[20] = 1 if cfg.get("vpot", False) else 0  # keep the 3D vector potential
     for b, bm in enumerate(cfg["beams"]):
         o = P_FIXED + B_NPAR * b
         p[o:o + 3] = bm["np"]

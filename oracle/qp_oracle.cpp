@@ -464,6 +464,47 @@ void bf(const T* cu, T* bxy, const T* ffc, const Grid& G) {
     for (int c = 1; c <= 3; ++c) bxy[G.g(3, c, k, nx + 1)] = T(0);
 }
 
+// PBPOISD23 isign = 1, fpois2d_lib77.f:1085-1133, as called by ivppoisd2
+// (fpois2d_class.f03:242-271) with ci = 1: the vector potential
+// a(kx,ky) = ci^2 g(kx,ky) s(kx,ky) cu(kx,ky), with the reference's mode rules
+// (ky = 0: y only; kx = 0: x only; ky = ny, kx = nx and (0,0): zero).
+template <class T>
+void vpot(const T* cu, T* a, const T* ffc, const Grid& G) {
+  int ny = G.ny, nx = G.nx;
+  T ci = T(1.0), ci2 = ci * ci;
+  for (int j = 1; j <= nx; ++j) {
+    if (j - 1 > 0) {
+      for (int k = 2; k <= ny; ++k) {
+        T at2 = ci2 * FRE(k, j);
+        T at1 = at2 * FIM(k, j);
+        a[G.g(3, 1, k, j)] = at1 * cu[G.g(3, 1, k, j)];
+        a[G.g(3, 2, k, j)] = at1 * cu[G.g(3, 2, k, j)];
+        a[G.g(3, 3, k, j)] = at1 * cu[G.g(3, 3, k, j)];
+      }
+      T at2 = ci2 * FRE(1, j);
+      T at1 = at2 * FIM(1, j);
+      a[G.g(3, 1, 1, j)] = T(0);
+      a[G.g(3, 2, 1, j)] = at1 * cu[G.g(3, 2, 1, j)];
+      a[G.g(3, 3, 1, j)] = T(0);
+    }
+    a[G.g(3, 1, ny + 1, j)] = T(0);
+    a[G.g(3, 2, ny + 1, j)] = T(0);
+    a[G.g(3, 3, ny + 1, j)] = T(0);
+  }
+  for (int k = 2; k <= ny; ++k) {
+    T at2 = ci2 * FRE(k, 1);
+    T at1 = at2 * FIM(k, 1);
+    a[G.g(3, 1, k, 1)] = at1 * cu[G.g(3, 1, k, 1)];
+    a[G.g(3, 2, k, 1)] = T(0);
+    a[G.g(3, 3, k, 1)] = T(0);
+  }
+  a[G.g(3, 1, 1, 1)] = T(0);
+  a[G.g(3, 2, 1, 1)] = T(0);
+  a[G.g(3, 3, 1, 1)] = T(0);
+  for (int k = 1; k <= ny + 1; ++k)
+    for (int c = 1; c <= 3; ++c) a[G.g(3, c, k, nx + 1)] = T(0);
+}
+
 // PBPOISD22N_QP isign = 1, fpois2d_lib77.f:1322-1421, as called by
 // jpbpoisd23n_qp (fpois2d_class.f03:444-495) with kxp2 = nx, ci = 1:
 // the transverse-B corrector.  dcu is modified in place.
@@ -1675,6 +1716,10 @@ void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
   }                                                                                     \
   extern "C" int oq_bf_##S(const T* cu, T* bxy, const T* ffc, int indx, int indy) {     \
     bf<T>(cu, bxy, ffc, Grid(indx, indy));                                              \
+    return 0;                                                                           \
+  }                                                                                     \
+  extern "C" int oq_vpot_##S(const T* cu, T* a, const T* ffc, int indx, int indy) {    \
+    vpot<T>(cu, a, ffc, Grid(indx, indy));                                              \
     return 0;                                                                           \
   }                                                                                     \
   extern "C" int oq_bfqp_##S(const T* cu, T* dcu, const T* amu, T* bxy, const T* ffc,   \

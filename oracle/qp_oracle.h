@@ -47,6 +47,7 @@ extern "C" {
   int oq_smooth_##S(const T* q, T* qs, const T* ffc, int indx, int indy);           \
   int oq_elf_##S(const T* q, T* fxy, const T* ffc, int indx, int indy);             \
   int oq_bf_##S(const T* cu, T* bxy, const T* ffc, int indx, int indy);             \
+  int oq_vpot_##S(const T* cu, T* a, const T* ffc, int indx, int indy);            \
   int oq_bfqp_##S(const T* cu, T* dcu, const T* amu, T* bxy, const T* ffc, T aa,    \
                   T dex, int indx, int indy);                                        \
   int oq_div_##S(const T* f, T* df, int ndim, int indx, int indy);                  \

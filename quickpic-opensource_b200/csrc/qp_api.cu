@@ -462,6 +462,10 @@ extern "C" int qp_field2d_bf(qp_field2d* s, qp_field2d* d) {
   if (s->dim != 3) return fail(s->ctx, __LINE__, "jpbpoisd23: invalid cu vector size");
   return kop(s->ctx, KOP_BF, s, d, 3, 3);
 }
+extern "C" int qp_field2d_vpot(qp_field2d* s, qp_field2d* d) {
+  if (s->dim != 3 || d->dim != 3) return fail(s->ctx, __LINE__, "ivpotd2: invalid vector size");
+  return kop(s->ctx, KOP_VPOT, s, d, 3, 3);
+}
 extern "C" int qp_field2d_div(qp_field2d* s, qp_field2d* d) { return kop(s->ctx, KOP_DIV, s, d, 2, 1); }
 extern "C" int qp_field2d_grad(qp_field2d* s, qp_field2d* d) { return kop(s->ctx, KOP_GRAD, s, d, 1, 2); }
 

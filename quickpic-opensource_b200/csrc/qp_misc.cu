@@ -66,6 +66,14 @@ __global__ void k_kpoint(int op, GridDims g, KCoef K, KPtrs in, KPtrs out, float
       out.p[1][o] = fy;
       break;
     }
+    case KOP_VPOT: {
+      float ax, ay, az;
+      k_vpot(K, kx, ky, in.p[0][o], in.p[1][o], in.p[2][o], &ax, &ay, &az);
+      out.p[0][o] = ax;
+      out.p[1][o] = ay;
+      out.p[2][o] = az;
+      break;
+    }
   }
 }
 

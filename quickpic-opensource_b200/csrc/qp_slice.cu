@@ -164,6 +164,13 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
     line[2][ky] = by;
     line[3][ky] = bz;
     if (b.q_in) line[8][ky] = k_smooth(K, kx, ky, line[8][ky]);
+    if (b.vpot_out[0]) {
+      float ax, ay, az;
+      k_vpot(K, kx, ky, cx, cy, cz, &ax, &ay, &az);
+      b.vpot_out[0][o] = ax;
+      b.vpot_out[1][o] = ay;
+      b.vpot_out[2][o] = az;
+    }
   }
   // relative change of B_perp for the convergence-controlled iteration
   r_num = warp_sum(r_num);

@@ -30,6 +30,7 @@ struct SliceB {
   float* out[4];
   const float* q_in;  // optional x-transformed q + cu_z (species2d%cbq)
   float* q_out;
+  float* vpot_out[3];  // optional: the vector potential of the pass's current (Fourier space)
   float* zero[8];     // real-space planes to clear for the next pass
   int nzero;
   // convergence-controlled loop: accumulate the relative change of B_perp,

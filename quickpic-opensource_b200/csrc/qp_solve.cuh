@@ -83,6 +83,29 @@ __device__ __forceinline__ void k_bf(const KCoef& K, int kx, int ky, float cux, 
   }
 }
 
+// The vector potential (field2d%vpot: PBPOISD23 isign = 1,
+// fpois2d_lib77.f:1085-1133, ci = 1): a = g s cu, with the reference's mode
+// rules (ky = 0: y only; kx = 0: x only; ky = ny, kx = nx and (0,0): zero).
+__device__ __forceinline__ void k_vpot(const KCoef& K, int kx, int ky, float cux, float cuy,
+                                       float cuz, float* ax, float* ay, float* az) {
+  *ax = 0.f;
+  *ay = 0.f;
+  *az = 0.f;
+  if (kx >= K.nx || ky >= K.ny) return;
+  if (kx > 0) {
+    const float at1 = QM(K.re(kx, ky), K.im(kx, ky));
+    if (ky > 0) {
+      *ax = QM(at1, cux);
+      *ay = QM(at1, cuy);
+      *az = QM(at1, cuz);
+    } else {
+      *ay = QM(at1, cuy);
+    }
+  } else if (ky > 0) {
+    *ax = QM(QM(K.re(0, ky), K.im(0, ky)), cux);
+  }
+}
+
 // The transverse-B corrector.  dcu is updated in place (the reference writes
 // the modified dcu back, and the slice loop extrapolates the current with it).
 __device__ __forceinline__ void k_bfqp(const KCoef& K, int kx, int ky, float aa, float idex,
@@ -157,6 +180,6 @@ __device__ __forceinline__ void k_assemble_mode(float ex, float ey, float ebx, f
 // standalone launches used by the class-level API
 int launch_kpoint(int op, const GridDims& g, const KCoef& K, float* const* in, float* const* out,
                   float aa, float dex, const DevStatus* st, cudaStream_t s);
-enum { KOP_POT = 0, KOP_SMOOTH, KOP_ELF, KOP_BF, KOP_BFQP, KOP_DIV, KOP_GRAD };
+enum { KOP_POT = 0, KOP_SMOOTH, KOP_ELF, KOP_BF, KOP_BFQP, KOP_DIV, KOP_GRAD, KOP_VPOT };
 
 }  // namespace qp

@@ -96,7 +96,8 @@ class _BeamDesc(C.Structure):
 
 class _SimDesc(C.Structure):
     _fields_ = [("iter", C.c_int), ("store3d", C.c_int), ("use_graphs", C.c_int),
-                ("dt", C.c_float), ("tol", C.c_float), ("reserved", C.c_int * 3)]
+                ("dt", C.c_float), ("tol", C.c_float), ("vpot", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class StepStats(C.Structure):
@@ -208,6 +209,9 @@ class Field2d:
 
     def bf(self, that):
         self._c(self.ctx._L.qp_field2d_bf(self.h, that.h))
+
+    def vpot(self, that):
+        self._c(self.ctx._L.qp_field2d_vpot(self.h, that.h))
 
     def div(self, that):
         self._c(self.ctx._L.qp_field2d_div(self.h, that.h))
@@ -407,10 +411,11 @@ class Simulation:
     """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
 
     def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False,
-                 dt=0.0, tol=0.0):
+                 dt=0.0, tol=0.0, vpot=False):
         d = _SimDesc()
         d.iter = iter  # passes per slice; with tol > 0 the most passes a slice may take
         d.tol = tol  # > 0: stop a slice's passes once |d epw| / |epw| <= tol
+        d.vpot = 1 if vpot else 0  # keep the 3D vector potential ("vpot")
         d.store3d = 1 if store3d else 0
         d.use_graphs = 1 if use_graphs else 0
         d.dt = dt  # 3D time step; > 0 ends every step with the beam push

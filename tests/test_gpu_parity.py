@@ -112,6 +112,7 @@ def test_kspace_solves(qp, ctx, oracle_mod):
         ("elf", fq, out2, lambda o: O.elf(np.asfortranarray(q), o, t, ix, iy), 2),
         ("grad", fq, out2, lambda o: O.grad(np.asfortranarray(q), o, ix, iy), 2),
         ("bf", fcu, out3, lambda o: O.bf(np.asfortranarray(cu), o, t, ix, iy), 3),
+        ("vpot", fcu, out3, lambda o: O.vpot(np.asfortranarray(cu), o, t, ix, iy), 3),
         ("div", fcu, out1, lambda o: O.div(np.asfortranarray(cu), o, ix, iy), 1),
     ]
     for name, src, dst, ref, dim in cases:
@@ -338,7 +339,7 @@ def _gpu_sim(qp, cfg, use_graphs=False, dt=0.0):
                                peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
     sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs,
-                        dt=dt, tol=cfg.get("tol", 0.0))
+                        dt=dt, tol=cfg.get("tol", 0.0), vpot=cfg.get("vpot", False))
     return c, sp, beams, sim
 
 
@@ -419,6 +420,26 @@ def test_convergence_controlled_step_matches_oracle(qp, oracle_mod):
     assert abs(st2.iterations - st.iterations) <= 4, (st2.iterations, st.iterations)
     assert st2.unconverged <= st.unconverged
     assert st2.kernels < st.kernels
+    sim.close()
+    c.close()
+
+
+def test_vpot3d_matches_oracle(qp, oracle_mod):
+    """The vector-potential diagnostic of the step (simulation_class.f03:711-716):
+    field2d%vpot of the last pass's current, fftkr, times -dex, per slice."""
+    O = oracle_mod
+    cfg = make_config(ind=(6, 6, 5), iter=2)
+    cfg["vpot"] = True
+    c, sp, beams, sim = _gpu_sim(qp, cfg)
+    sim.step3d()
+    o64 = O.Sim(cfg, np.float64)
+    o64.begin3d()
+    for j in range(1, 33):
+        o64.slice(j)
+    va = sim.get_3d("vpot")
+    ova = o64.get("vpot3d").reshape(va.shape, order="F")
+    assert np.abs(ova).max() > 0
+    assert rel_l2(va, ova) < 1e-4
     sim.close()
     c.close()
 
