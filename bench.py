@@ -48,6 +48,13 @@ CONFIGS = {
                                peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                                sigma=[0.3, 0.3, 0.6],
                                sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the medium case with the reference's fixed 2 B passes per slice (no tolerance)
+    "medium_fixed2": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2, dt=10.0,
+                          species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                          beams=[dict(np=[256, 256, 128], q=-1.0, m=1.0, gamma=20000.0,
+                                      peak_density=4.0, quiet_start=True,
+                                      center=[0.0, 0.0, 3.0], sigma=[0.3, 0.3, 0.6],
+                                      sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the medium transverse grid with 64 slices: the profiling case (< 1 GB on the device)
     "prof": dict(grid=dict(ind=[9, 9, 6], box=BOX), iter=16, tol=1e-4, dt=10.0,
                  species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),

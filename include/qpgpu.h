@@ -123,14 +123,35 @@ int qp_field2d_ag(qp_field2d* f); /* acopyguard: row 0 += row ny (ufield2d_lib.f
 
 /* ------------------------------------------------------------ species2d */
 
-/* Plasma species of profile 0 (uniform, fdist2d_000, fdist2d_class.f03:164-316)
- * with the keys species(i).{ppc, q, m, density}; xtras is part2d's buffer
- * headroom (0.2 in the reference, part2d_class.f03:62). */
+/* Plasma species (species(i) of the input, fdist2d_class.f03) with the keys
+ * {profile, ppc, q, m, density}; xtras is part2d's buffer headroom (0.2 in
+ * the reference, part2d_class.f03:62).  profile selects the loader:
+ *   0  uniform                        (fdist2d_000, 212-316)
+ *   10 elliptic hollow channel        (fdist2d_010, 318-523): the particles
+ *      on or between the inner and the outer ellipse about center
+ *   11 Gaussian ring                  (fdist2d_011, 525-711): charge weight
+ *      exp(-(r - radius)^2 / (2 width^2))
+ *   12 tabulated radial density f(r)  (fdist2d_012, 713-950), linear between
+ *      the nr points (r[i], fr[i]), no particles outside [r[0], r[nr-1]]
+ * Lengths (center, radii, width, r) are in the units of the box.  With ns > 0
+ * the density is also scaled by the piecewise-linear longitudinal profile
+ * (s[i], fs[i]) at the s given to qp_species_create / qp_species_renew
+ * (longitudinal_profile = 'piecewise'); the arrays are read during those calls
+ * only.  Unused fields may be zero. */
 typedef struct {
   int profile;
   int ppc[2];
   float q, m, density;
   float xtras;
+  float center[2];                        /* 10, 11, 12 */
+  float inner_radius[2], outer_radius[2]; /* 10: x and y radii */
+  float radius, width;                    /* 11 */
+  int nr;                                 /* 12 */
+  const float* r;
+  const float* fr;
+  int ns;                                 /* longitudinal piecewise density */
+  const float* s;
+  const float* fs;
 } qp_species_desc;
 
 /* species2d%new (species2d_class.f03:74-118): loads and bins the particles

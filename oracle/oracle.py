@@ -171,6 +171,23 @@ def dist2d_000(indx, indy, xppc, yppc, q=-1.0, den=1.0, dtype=np.float32):
     return part[:, : npp.value].copy(order="F")
 
 
+def dist2d_prof(indx, indy, box, xppc, yppc, profile, q=-1.0, den=1.0, center=(0.0, 0.0),
+                inner_radius=(0.0, 0.0), outer_radius=(0.0, 0.0), radius=0.0, width=0.0,
+                r=(), fr=(), s=0.0, long_s=(), long_fs=(), dtype=np.float32):
+    """The profile-10/11/12 (and 0) loaders with a piecewise longitudinal factor."""
+    nx, ny = 1 << indx, 1 << indy
+    npmax = xppc * yppc * nx * ny
+    pr = np.array([profile, xppc, yppc, q, den, box[0][0], box[0][1], box[1][0], box[1][1],
+                   indx, indy, center[0], center[1], inner_radius[0], inner_radius[1],
+                   outer_radius[0], outer_radius[1], radius, width, s, len(r), len(long_s)]
+                  + list(r) + list(fr) + list(long_s) + list(long_fs), dtype=dtype)
+    part = np.zeros((8, npmax), dtype=dtype, order="F")
+    npp = C.c_int(0)
+    rc = _call("oq_dist2d_prof", dtype, part, npmax, C.byref(npp), pr)
+    assert rc == 0, rc
+    return part[:, : npp.value].copy(order="F")
+
+
 def bin_particles(part, indx, indy, xtras=0.2, nppmx0=None):
     """PPDBLKP2L + PPPMOVIN2L: linear part(8, n) -> (ppart, kpic, nppmx0)."""
     dtype = part.dtype

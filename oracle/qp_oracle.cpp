@@ -1390,6 +1390,97 @@ int dist2d_000(T* part, int npmax, int* npp, int xppc, int yppc, T qsign_q, T de
   return 0;
 }
 
+// The other plasma loaders of fdist2d_class.f03 for one rank (noff = 0 < ny):
+// init_fdist2d_010/011/012 (318-387, 525-590, 713-776) convert the lengths to
+// cells, dist2d_010 (389-523) keeps the particles on or between two ellipses,
+// dist2d_011 (592-711) weights the charge by a Gaussian ring and dist2d_012
+// (778-950) by a piecewise-linear f(r); all take the longitudinal factor
+// den_temp (421-438) of a 'piecewise' profile.  pr = profile, xppc, yppc, q,
+// den, box x min/max, box y min/max, indx, indy, center x/y, inner radius x/y,
+// outer radius x/y, radius, width, s, nr, ns, then r(nr), fr(nr), s(ns), fs(ns).
+template <class T>
+int dist2d_prof(T* part, int npmax, int* npp, const T* pr) {
+  const int npf = (int)pr[0], xppc = (int)pr[1], yppc = (int)pr[2];
+  const T q = pr[3], den = pr[4];
+  const int indx = (int)pr[9], indy = (int)pr[10];
+  const Grid G(indx, indy);
+  const T dx = (pr[6] - pr[5]) / T(1 << indx), dy = (pr[8] - pr[7]) / T(1 << indy);
+  const T cx = (pr[11] - pr[5]) / dx, cy = (pr[12] - pr[7]) / dy;
+  const T irx = pr[13] / dx, iry = pr[14] / dy, orx = pr[15] / dx, ory = pr[16] / dy;
+  const T r0 = pr[17] / dx, sigr = pr[18] / dx;
+  const T s = pr[19];
+  const int nr = (int)pr[20], ns = (int)pr[21];
+  std::vector<T> r(nr), fr(nr), ls(ns), lfs(ns);
+  for (int k = 0; k < nr; ++k) {
+    r[k] = pr[22 + k] / dx;
+    fr[k] = pr[22 + nr + k];
+  }
+  for (int k = 0; k < ns; ++k) {
+    ls[k] = pr[22 + 2 * nr + k];
+    lfs[k] = pr[22 + 2 * nr + ns + k];
+  }
+  T den_temp = T(1.0);
+  if (ns > 0) {
+    if (s < ls[0] || s > ls[ns - 1]) return -2;
+    for (int i = 2; i <= ns; ++i) {
+      if (ls[i - 1] < ls[i - 2]) return -3;
+      if (s <= ls[i - 1]) {
+        den_temp = lfs[i - 2] + (lfs[i - 1] - lfs[i - 2]) / (ls[i - 1] - ls[i - 2]) *
+                                    (s - ls[i - 2]);
+        break;
+      }
+    }
+  }
+  const T qm = den_temp * den * q / std::abs(q) / T(xppc) / T(yppc);
+  const T iirx2 = T(1.0) / (irx * irx), iiry2 = T(1.0) / (iry * iry);
+  const T iorx2 = T(1.0) / (orx * orx), iory2 = T(1.0) / (ory * ory);
+  const T isigr2 = T(0.5) / (sigr * sigr);
+  int nps = 1;
+  for (int i = 2; i <= G.nx - 1; ++i)
+    for (int j = 2; j <= G.ny; ++j)
+      for (int ix = 0; ix <= xppc - 1; ++ix)
+        for (int iy = 0; iy <= yppc - 1; ++iy) {
+          const T x = (T(ix) + T(0.5)) / T(xppc) + T(i) - T(1);
+          const T y = (T(iy) + T(0.5)) / T(yppc) + T(j) - T(1) + T(0);
+          T qp = qm;
+          if (npf == 10) {
+            if (((x - cx) * (x - cx) * iirx2 + (y - cy) * (y - cy) * iiry2 < T(1)) ||
+                ((x - cx) * (x - cx) * iorx2 + (y - cy) * (y - cy) * iory2 > T(1)))
+              continue;
+          } else if (npf == 11) {
+            const T rr = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
+            qp = qm * std::exp(-(rr - r0) * (rr - r0) * isigr2);
+          } else if (npf == 12) {
+            const T rr = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
+            if (rr < r[0] || rr > r[nr - 1]) continue;
+            for (int ii = 2; ii <= nr; ++ii) {
+              if (r[ii - 1] <= r[ii - 2]) return -4;
+              if (rr <= r[ii - 1]) {
+                den_temp = fr[ii - 2] + (fr[ii - 1] - fr[ii - 2]) / (r[ii - 1] - r[ii - 2]) *
+                                            (rr - r[ii - 2]);
+                break;
+              }
+            }
+            qp = qm * den_temp;
+          } else if (npf != 0) {
+            return -5;
+          }
+          if (nps > npmax) return -1;
+          T* pt = &part[8 * (size_t)(nps - 1)];
+          pt[0] = x;
+          pt[1] = y;
+          pt[2] = T(0.0);
+          pt[3] = T(0.0);
+          pt[4] = T(0.0);
+          pt[5] = T(1.0);
+          pt[6] = T(1.0);
+          pt[7] = qp;
+          nps = nps + 1;
+        }
+  *npp = nps - 1;
+  return 0;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- ranorm
@@ -1787,6 +1878,9 @@ void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
   extern "C" int oq_dist2d_000_##S(T* part, int npmax, int* npp, int xppc, int yppc,    \
                                    T qm, T den, int indx, int indy) {                   \
     return dist2d_000<T>(part, npmax, npp, xppc, yppc, qm, den, Grid(indx, indy));      \
+  }                                                                                     \
+  extern "C" int oq_dist2d_prof_##S(T* part, int npmax, int* npp, const T* pr) {       \
+    return dist2d_prof<T>(part, npmax, npp, pr);                                        \
   }                                                                                     \
   extern "C" int oq_beam_qm_##S(T q, T np, const T* sig, const T* lo, const T* hi,      \
                                 int indx, int indy, int indz, int npx, int npy,         \

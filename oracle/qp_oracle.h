@@ -78,6 +78,7 @@ extern "C" {
   int oq_pppcheck2l_##S(const T* ppart, const int* kpic, int nppmx, int indx,       \
                         int indy);                                                   \
   /* loaders */                                                                      \
+  int oq_dist2d_prof_##S(T* part, int npmax, int* npp, const T* pr);               \
   int oq_dist2d_000_##S(T* part, int npmax, int* npp, int xppc, int yppc, T qm,     \
                         T den, int indx, int indy);                                  \
   int oq_beam_qm_##S(T q, T np, const T* sig, const T* box_lo, const T* box_hi,     \

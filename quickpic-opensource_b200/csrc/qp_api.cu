@@ -93,6 +93,7 @@ struct qp_species {
   float* q3 = nullptr;         // (nz+1) real planes
   float* q3_first = nullptr;   // slice-1 plane after renew (pristine)
   int regrowths = 0;
+  PlasmaProfile prof;          // the loader's profile, lengths in cells
 };
 
 struct qp_beam {
@@ -674,52 +675,117 @@ static int species_background(qp_species* sp) {
   return 0;
 }
 
-extern "C" int qp_species_create(qp_ctx* ctx, const qp_species_desc* d, float s,
-                                 qp_species** out) {
-  (void)s;
-  if (!ctx || !d || !out) return fail(ctx, __LINE__, "null argument");
-  if (d->profile != 0) return fail(ctx, __LINE__, "only the uniform plasma profile 0 is supported");
-  if (d->ppc[0] < 1 || d->ppc[1] < 1) return fail(ctx, __LINE__, "invalid ppc");
-  qp_species* sp = new qp_species();
-  sp->ctx = ctx;
-  sp->d = *d;
-  sp->qbm = d->q / d->m;
-  sp->dt = ctx->dxi;
+// The profile of a species descriptor with its lengths in cells, converted
+// in FP32 as init_fdist2d_0xx does (fdist2d_class.f03:164-210, 318-387,
+// 525-590, 713-776): c = (center - box min) / (box length / 2^ind).
+static int species_profile(qp_ctx* ctx, const qp_species_desc* d, PlasmaProfile* p) {
+  p->profile = d->profile;
+  p->xppc = d->ppc[0];
+  p->yppc = d->ppc[1];
+  p->q = d->q;
+  p->den = d->density;
+  const float xmin = (float)ctx->box[0][0], xmax = (float)ctx->box[0][1];
+  const float ymin = (float)ctx->box[1][0], ymax = (float)ctx->box[1][1];
+  const float dx = (xmax - xmin) / (float)(1 << ctx->g.indx);
+  const float dy = (ymax - ymin) / (float)(1 << ctx->g.indy);
+  p->cx = (d->center[0] - xmin) / dx;
+  p->cy = (d->center[1] - ymin) / dy;
+  p->irx = d->inner_radius[0] / dx;
+  p->iry = d->inner_radius[1] / dy;
+  p->orx = d->outer_radius[0] / dx;
+  p->ory = d->outer_radius[1] / dy;
+  p->r0 = d->radius / dx;
+  p->sigr = d->width / dx;
+  if (d->profile == 12) {
+    if (d->nr < 2 || !d->r || !d->fr) return fail(ctx, __LINE__, "profile 12 needs nr >= 2 points");
+    p->r.resize(d->nr);
+    p->fr.assign(d->fr, d->fr + d->nr);
+    for (int k = 0; k < d->nr; ++k) p->r[k] = d->r[k] / dx;
+  }
+  if (d->ns > 0) {
+    if (!d->s || !d->fs) return fail(ctx, __LINE__, "longitudinal profile: null arrays");
+    p->s.assign(d->s, d->s + d->ns);
+    p->fs.assign(d->fs, d->fs + d->ns);
+  }
+  if (d->profile == 10 && !(p->irx > 0.f && p->iry > 0.f && p->orx > 0.f && p->ory > 0.f))
+    return fail(ctx, __LINE__, "profile 10 needs positive inner and outer radii");
+  if (d->profile == 11 && !(p->sigr > 0.f)) return fail(ctx, __LINE__, "profile 11 needs width > 0");
+  return 0;
+}
+
+// Loads the species' profile at s (PPDBLKP2L: particles per tile and nppmx;
+// PPPMOVIN2L: a stable copy into the tiles) into the pristine buffer P0 and
+// the live buffer A, growing the buffers when the load needs more room.
+static int species_load(qp_species* sp, float s) {
+  qp_ctx* ctx = sp->ctx;
   const GridDims& g = ctx->g;
   const TileGeom& tg = ctx->tg;
   std::vector<float> c[8];
-  sp->np = plasma_uniform(g.nx, g.ny, d->ppc[0], d->ppc[1], d->q, d->density, c);
-  // PPDBLKP2L: particles per tile, nppmx; PPPMOVIN2L: stable copy into tiles
-  std::vector<int> cnt(tg.ntiles, 0), tile(sp->np);
-  for (long long n = 0; n < sp->np; ++n) {
+  std::string err;
+  const long long np = plasma_load(sp->prof, g.nx, g.ny, s, c, &err);
+  if (np < 0) return fail(ctx, __LINE__, "plasma loader: " + err);
+  sp->np = np;
+  std::vector<int> cnt(tg.ntiles, 0), tile(np);
+  for (long long n = 0; n < np; ++n) {
     const int tx = (int)c[0][n] / TILE, ty = (int)c[1][n] / TILE;
     tile[n] = tx + tg.mx1 * ty;
     cnt[tile[n]]++;
   }
   int nppmx = 0;
   for (int v : cnt) nppmx = std::max(nppmx, v);
-  const float xtras = d->xtras > 0 ? d->xtras : 0.2f;
-  sp->nppmx0 = (int)((1.0f + xtras) * (float)nppmx);
-  if (part_alloc(&sp->A, tg.ntiles, std::max(sp->nppmx0, 1)) ||
-      part_alloc(&sp->B, tg.ntiles, std::max(sp->nppmx0, 1)) ||
-      part_alloc(&sp->P0, tg.ntiles, std::max(sp->nppmx0, 1)))
-    return fail(ctx, __LINE__, "out of device memory (particles)");
-  const int cap = sp->P0.cap;  // rounded up to a multiple of 4 by part_alloc
-  const int capin = std::max(64, (int)(xtras * (float)nppmx));
-  if (inbox_alloc(&sp->ib, tg.ntiles, capin)) return fail(ctx, __LINE__, "out of device memory");
-  {
-    std::vector<float> h((size_t)tg.ntiles * cap, 0.f);
-    std::vector<int> pos(tg.ntiles, 0);
-    std::vector<long long> slot(sp->np);
-    for (long long n = 0; n < sp->np; ++n) slot[n] = (long long)tile[n] * cap + pos[tile[n]]++;
-    for (int k = 0; k < NCOMP; ++k) {
-      std::fill(h.begin(), h.end(), 0.f);
-      for (long long n = 0; n < sp->np; ++n) h[slot[n]] = c[k][n];
-      CK(cudaMemcpy(sp->P0.c[k], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+  const float xtras = sp->d.xtras > 0 ? sp->d.xtras : 0.2f;
+  const int nppmx0 = (int)((1.0f + xtras) * (float)nppmx);
+  if (sp->P0.cap == 0 || nppmx0 > sp->P0.cap) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int want = std::max({nppmx0, sp->A.cap, 1});
+    part_free(&sp->P0);
+    if (part_alloc(&sp->P0, tg.ntiles, std::max(nppmx0, 1)))
+      return fail(ctx, __LINE__, "out of device memory (particles)");
+    if (sp->A.cap < sp->P0.cap) {
+      part_free(&sp->A);
+      part_free(&sp->B);
+      if (part_alloc(&sp->A, tg.ntiles, want) || part_alloc(&sp->B, tg.ntiles, want))
+        return fail(ctx, __LINE__, "out of device memory (particles)");
     }
-    CK(cudaMemcpy(sp->P0.count, cnt.data(), sizeof(int) * tg.ntiles, cudaMemcpyHostToDevice));
   }
-  if (part_copy(ctx, sp->A, sp->P0)) return -1;
+  sp->nppmx0 = std::max(sp->nppmx0, nppmx0);
+  if (!sp->ib.count) {
+    const int capin = std::max(64, (int)(xtras * (float)nppmx));
+    if (inbox_alloc(&sp->ib, tg.ntiles, capin)) return fail(ctx, __LINE__, "out of device memory");
+  }
+  const int cap = sp->P0.cap;  // rounded up to a multiple of 4 by part_alloc
+  std::vector<float> h((size_t)tg.ntiles * cap, 0.f);
+  std::vector<int> pos(tg.ntiles, 0);
+  std::vector<long long> slot(np);
+  for (long long n = 0; n < np; ++n) slot[n] = (long long)tile[n] * cap + pos[tile[n]]++;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < NCOMP; ++k) {
+    std::fill(h.begin(), h.end(), 0.f);
+    for (long long n = 0; n < np; ++n) h[slot[n]] = c[k][n];
+    CK(cudaMemcpy(sp->P0.c[k], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(sp->P0.count, cnt.data(), sizeof(int) * tg.ntiles, cudaMemcpyHostToDevice));
+  for (int k = 0; k < NCOMP; ++k)
+    launch_lin((long long)tg.ntiles * sp->A.cap, sp->A.c[k], nullptr, nullptr, 0.f, LIN_FILL,
+               ctx->st, ctx->stream);
+  return part_copy(ctx, sp->A, sp->P0);
+}
+
+extern "C" int qp_species_create(qp_ctx* ctx, const qp_species_desc* d, float s,
+                                 qp_species** out) {
+  if (!ctx || !d || !out) return fail(ctx, __LINE__, "null argument");
+  if (d->ppc[0] < 1 || d->ppc[1] < 1) return fail(ctx, __LINE__, "invalid ppc");
+  qp_species* sp = new qp_species();
+  sp->ctx = ctx;
+  sp->d = *d;
+  sp->d.r = sp->d.fr = sp->d.s = sp->d.fs = nullptr;  // the arrays are copied into prof
+  sp->qbm = d->q / d->m;
+  sp->dt = ctx->dxi;
+  const GridDims& g = ctx->g;
+  if (species_profile(ctx, d, &sp->prof) || species_load(sp, s)) {
+    qp_species_destroy(sp);
+    return -1;
+  }
   sp->q = field_new(ctx, 1, 0);
   sp->qn = field_new(ctx, 1, 0);
   sp->cusp = field_new(ctx, 3, 0);
@@ -759,11 +825,17 @@ extern "C" int qp_species_destroy(qp_species* sp) {
   return 0;
 }
 
-// The uniform profile is deterministic, so renew restores the pristine copy of
+// A transverse profile is deterministic, so renew restores the pristine copy of
 // the loaded, binned plasma and its background (same bits as a fresh load).
+// With a longitudinal profile the density depends on s: the plasma is loaded
+// afresh at s (species2d%renew, species2d_class.f03:138-164).
 extern "C" int qp_species_renew(qp_species* sp, float s) {
-  (void)s;
   qp_ctx* ctx = sp->ctx;
+  if (!sp->prof.fs.empty()) {
+    if (species_load(sp, s) || species_background(sp)) return -1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+  }
   if (sp->A.cap < sp->P0.cap) return fail(ctx, __LINE__, "renew: capacity shrank");
   for (int c = 0; c < NCOMP; ++c)
     launch_lin((long long)ctx->tg.ntiles * sp->A.cap, sp->A.c[c], nullptr, nullptr, 0.f, LIN_FILL,

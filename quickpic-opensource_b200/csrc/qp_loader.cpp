@@ -95,6 +95,94 @@ long long plasma_uniform(int nx, int ny, int xppc, int yppc, float q, float den,
   return n;
 }
 
+// The longitudinal factor den_temp of dist2d_0xx (fdist2d_class.f03:421-438):
+// 1 without a profile, else linear between the points (s[i], fs[i]).
+static bool longitudinal(const PlasmaProfile& p, float s, float* den, std::string* err) {
+  *den = 1.0f;
+  const int n = (int)p.fs.size();
+  if (n == 0) return true;
+  if ((int)p.s.size() != n) {
+    *err = "piecewise_density and piecewise_s have different sizes";
+    return false;
+  }
+  if (s < p.s[0] || s > p.s[n - 1]) {
+    *err = "The s is out of the bound!";
+    return false;
+  }
+  for (int i = 1; i < n; ++i) {
+    if (p.s[i] < p.s[i - 1]) {
+      *err = "s is not monotonically increasing!";
+      return false;
+    }
+    if (s <= p.s[i]) {
+      *den = p.fs[i - 1] + (p.fs[i] - p.fs[i - 1]) / (p.s[i] - p.s[i - 1]) * (s - p.s[i - 1]);
+      break;
+    }
+  }
+  return true;
+}
+
+long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s,
+                      std::vector<float> (&c)[8], std::string* err) {
+  float den_temp;
+  if (!longitudinal(p, s, &den_temp, err)) return -1;
+  const float qm = den_temp * p.den * p.q / std::fabs(p.q) / (float)p.xppc / (float)p.yppc;
+  const int nr = (int)p.r.size();
+  if (p.profile == 12) {
+    if (nr < 2 || (int)p.fr.size() != nr) {
+      *err = "The piecewise_radial_density and r array have different sizes!";
+      return -1;
+    }
+    for (int k = 1; k < nr; ++k)
+      if (p.r[k] <= p.r[k - 1]) {
+        *err = "r is not monotonically increasing!";
+        return -1;
+      }
+  } else if (p.profile != 0 && p.profile != 10 && p.profile != 11) {
+    *err = "Invalid species profile number: " + std::to_string(p.profile);
+    return -1;
+  }
+  // fdist2d_010: reciprocal squared radii; fdist2d_011: 0.5 / sigr^2
+  const float iirx2 = 1.0f / (p.irx * p.irx), iiry2 = 1.0f / (p.iry * p.iry);
+  const float iorx2 = 1.0f / (p.orx * p.orx), iory2 = 1.0f / (p.ory * p.ory);
+  const float isigr2 = 0.5f / (p.sigr * p.sigr);
+  for (auto& v : c) v.clear();
+  for (int i = 2; i <= nx - 1; ++i)
+    for (int j = 2; j <= ny; ++j)
+      for (int ix = 0; ix < p.xppc; ++ix)
+        for (int iy = 0; iy < p.yppc; ++iy) {
+          const float x = ((float)ix + 0.5f) / (float)p.xppc + (float)i - 1.0f;
+          const float y = ((float)iy + 0.5f) / (float)p.yppc + (float)j - 1.0f + 0.0f;
+          float q = qm;
+          if (p.profile == 10) {
+            const float dx2 = (x - p.cx) * (x - p.cx), dy2 = (y - p.cy) * (y - p.cy);
+            if (dx2 * iirx2 + dy2 * iiry2 < 1.0f || dx2 * iorx2 + dy2 * iory2 > 1.0f) continue;
+          } else if (p.profile == 11) {
+            const float rr = std::sqrt((x - p.cx) * (x - p.cx) + (y - p.cy) * (y - p.cy));
+            q = qm * std::exp(-((rr - p.r0) * (rr - p.r0)) * isigr2);
+          } else if (p.profile == 12) {
+            const float rr = std::sqrt((x - p.cx) * (x - p.cx) + (y - p.cy) * (y - p.cy));
+            if (rr < p.r[0] || rr > p.r[nr - 1]) continue;
+            float f = den_temp;
+            for (int k = 1; k < nr; ++k)
+              if (rr <= p.r[k]) {
+                f = p.fr[k - 1] + (p.fr[k] - p.fr[k - 1]) / (p.r[k] - p.r[k - 1]) * (rr - p.r[k - 1]);
+                break;
+              }
+            q = qm * f;
+          }
+          c[0].push_back(x);
+          c[1].push_back(y);
+          c[2].push_back(0.f);
+          c[3].push_back(0.f);
+          c[4].push_back(0.f);
+          c[5].push_back(1.f);
+          c[6].push_back(1.f);
+          c[7].push_back(q);
+        }
+  return (long long)c[0].size();
+}
+
 float beam_charge(float q, float peak, const float sig[3], const float lo[3], const float hi[3],
                   int indx, int indy, int indz, int npx, int npy, int npz) {
   const float dx = (hi[0] - lo[0]) / (float)(1 << indx);

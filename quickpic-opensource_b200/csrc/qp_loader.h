@@ -1,6 +1,7 @@
 // qp_loader.h -- host-side initial conditions and tables (see qp_loader.cpp).
 #pragma once
 
+#include <string>
 #include <vector>
 
 namespace qp {
@@ -17,6 +18,25 @@ struct Ranorm {
 // x, y, px, py, pz, p6, p7, q in the loader's order.
 long long plasma_uniform(int nx, int ny, int xppc, int yppc, float q, float den,
                          std::vector<float> (&c)[8]);
+
+// A plasma profile with its lengths already in cells (the init_fdist2d_0xx
+// conversions): profile 0, 10, 11 or 12 (see qp_species_desc).
+struct PlasmaProfile {
+  int profile = 0;
+  int xppc = 1, yppc = 1;
+  float q = -1.f, den = 1.f;
+  float cx = 0.f, cy = 0.f;
+  float irx = 0.f, iry = 0.f, orx = 0.f, ory = 0.f;  // 10
+  float r0 = 0.f, sigr = 0.f;                       // 11
+  std::vector<float> r, fr;                         // 12
+  std::vector<float> s, fs;                         // longitudinal piecewise
+};
+
+// Loads profile p at propagation distance s (dist2d_0xx for one rank:
+// cells i = 2..nx-1, j = 2..ny, order i, j, ix, iy).  Returns the number of
+// particles, or -1 with a message in *err.
+long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s,
+                      std::vector<float> (&c)[8], std::string* err);
 
 struct BeamLoad {
   int npx, npy, npz, nx, ny, nz;

@@ -84,7 +84,11 @@ class _GridDesc(C.Structure):
 
 class _SpeciesDesc(C.Structure):
     _fields_ = [("profile", C.c_int), ("ppc", C.c_int * 2), ("q", C.c_float), ("m", C.c_float),
-                ("density", C.c_float), ("xtras", C.c_float)]
+                ("density", C.c_float), ("xtras", C.c_float), ("center", C.c_float * 2),
+                ("inner_radius", C.c_float * 2), ("outer_radius", C.c_float * 2),
+                ("radius", C.c_float), ("width", C.c_float),
+                ("nr", C.c_int), ("r", C.POINTER(C.c_float)), ("fr", C.POINTER(C.c_float)),
+                ("ns", C.c_int), ("s", C.POINTER(C.c_float)), ("fs", C.POINTER(C.c_float))]
 
 
 class _BeamDesc(C.Structure):
@@ -267,13 +271,37 @@ class Field2d:
 
 
 class Species2d:
-    """species2d with a uniform (profile 0) plasma."""
+    """species2d: plasma of profile 0 (uniform), 10 (elliptic hollow channel: center,
+    inner_radius, outer_radius), 11 (Gaussian ring: center, radius, width) or 12
+    (tabulated radial density: center, r, fr), optionally scaled by a
+    piecewise-linear longitudinal density (long_s, long_fs) at propagation
+    distance s.  Lengths are in the units of the box."""
 
-    def __init__(self, ctx: Context, ppc=(2, 2), q=-1.0, m=1.0, density=1.0, xtras=0.2, s=0.0):
+    def __init__(self, ctx: Context, ppc=(2, 2), q=-1.0, m=1.0, density=1.0, xtras=0.2, s=0.0,
+                 profile=0, center=(0.0, 0.0), inner_radius=(0.0, 0.0),
+                 outer_radius=(0.0, 0.0), radius=0.0, width=0.0, r=None, fr=None,
+                 long_s=None, long_fs=None):
         d = _SpeciesDesc()
-        d.profile = 0
+        d.profile = profile
         d.ppc[0], d.ppc[1] = ppc
         d.q, d.m, d.density, d.xtras = q, m, density, xtras
+        d.center[0], d.center[1] = center
+        d.inner_radius[0], d.inner_radius[1] = inner_radius
+        d.outer_radius[0], d.outer_radius[1] = outer_radius
+        d.radius, d.width = radius, width
+        keep = []  # the arrays must live through the create call
+
+        def arr(v):
+            a = np.ascontiguousarray(v, dtype=np.float32)
+            keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_float)), len(a)
+
+        if r is not None:
+            d.r, d.nr = arr(r)
+            d.fr, _ = arr(fr)
+        if long_s is not None:
+            d.s, d.ns = arr(long_s)
+            d.fs, _ = arr(long_fs)
         h = C.c_void_p()
         ctx._check(ctx._L.qp_species_create(ctx.h, C.byref(d), C.c_float(s), C.byref(h)))
         self.ctx, self.h = ctx, h

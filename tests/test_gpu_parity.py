@@ -137,6 +137,42 @@ def test_kspace_solves(qp, ctx, oracle_mod):
     assert np.array_equal(fb.get_ks(), b_ref)
 
 
+_PROFILES = [
+    dict(profile=10, center=(0.5, -0.5), inner_radius=(1.0, 2.0), outer_radius=(3.0, 4.0)),
+    dict(profile=11, center=(0.3, 0.2), radius=2.0, width=0.5),
+    dict(profile=12, center=(0.0, 0.0), r=(1.0, 2.0, 4.0), fr=(0.0, 1.0, 0.5)),
+    dict(profile=0, s=5.0, long_s=(0.0, 10.0), long_fs=(1.0, 3.0)),
+]
+
+
+@pytest.mark.parametrize("kw", _PROFILES, ids=["hollow", "ring", "f(r)", "longitudinal"])
+def test_plasma_profiles_load_like_oracle(qp, ctx, oracle_mod, kw):
+    """The engine's loader and binning of profiles 10, 11, 12 and of a piecewise
+    longitudinal density give the particles of the oracle's restatement, bit for
+    bit, tile by tile; renew at another s reloads the longitudinal density."""
+    O = oracle_mod
+    ix, iy = ctx.indx, ctx.indy
+    box = [[-6.0, 6.0], [-6.0, 6.0]]
+    sp = qp.Species2d(ctx, ppc=(2, 2), **kw)
+    ok = {k: v for k, v in kw.items() if k not in ("profile",)}
+    part = O.dist2d_prof(ix, iy, box, 2, 2, kw["profile"], dtype=np.float32, **ok)
+    pp, kp, _ = O.bin_particles(part, ix, iy)
+    gp, gk = sp.get_particles(max(sp.nppmx, pp.shape[1]))
+    assert np.array_equal(gk, kp)
+    for t in range(len(kp)):
+        assert np.array_equal(gp[:, : kp[t], t], pp[:, : kp[t], t]), t
+    if "long_s" in kw:
+        sp.renew(7.5)
+        ok["s"] = 7.5
+        part = O.dist2d_prof(ix, iy, box, 2, 2, kw["profile"], dtype=np.float32, **ok)
+        pp, kp, _ = O.bin_particles(part, ix, iy)
+        gp, gk = sp.get_particles(max(sp.nppmx, pp.shape[1]))
+        assert np.array_equal(gk, kp)
+        assert np.array_equal(gp[7, : kp[0], 0], pp[7, : kp[0], 0])
+        assert np.allclose(gp[7, : kp[0], 0], -0.25 * 2.5)
+    sp.close()
+
+
 def _particles(O, ix, iy, seed, jitter=0.2, pscale=0.05):
     part = O.dist2d_000(ix, iy, 2, 2, dtype=np.float32)
     rng = np.random.default_rng(seed)

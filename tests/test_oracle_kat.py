@@ -208,6 +208,40 @@ def test_fp32_oracle_tracks_fp64(oracle_mod):
     assert np.abs(s64.get("psi")).max() > 1e-3  # the beam drove a wake
 
 
+def test_plasma_profile_loaders(oracle_mod):
+    """fdist2d_010/011/012 and the piecewise longitudinal factor (the oracle's
+    restatement): profile 0 through the general loader is dist2d_000; 10 keeps
+    the particles on or between the two ellipses; 11 weights the charge by the
+    Gaussian ring; 12 interpolates f(r); the longitudinal factor scales q."""
+    O = oracle_mod
+    ix = iy = 6
+    box = [[-6.0, 6.0], [-6.0, 6.0]]
+    dx = 12.0 / 64
+    for dt in (np.float32, np.float64):
+        p0 = O.dist2d_prof(ix, iy, box, 2, 2, 0, dtype=dt)
+        assert np.array_equal(p0, O.dist2d_000(ix, iy, 2, 2, dtype=dt))
+    p = O.dist2d_prof(ix, iy, box, 2, 2, 10, center=(0.5, -0.5), inner_radius=(1.0, 2.0),
+                      outer_radius=(3.0, 4.0), dtype=np.float64)
+    ex = (p[0] - (0.5 + 6.0) / dx) * dx
+    ey = (p[1] - (-0.5 + 6.0) / dx) * dx
+    assert 0 < p.shape[1] < p0.shape[1]
+    assert np.all(ex ** 2 / 1.0 + ey ** 2 / 4.0 >= 1 - 1e-9)
+    assert np.all(ex ** 2 / 9.0 + ey ** 2 / 16.0 <= 1 + 1e-9)
+    p = O.dist2d_prof(ix, iy, box, 2, 2, 11, center=(0.0, 0.0), radius=2.0, width=0.5,
+                      dtype=np.float64)
+    assert p.shape == p0.shape
+    rr = np.hypot(p[0] - 32.0, p[1] - 32.0) * dx
+    assert np.allclose(p[7], -0.25 * np.exp(-((rr - 2.0) ** 2) / (2 * 0.5 ** 2)), rtol=1e-12)
+    p = O.dist2d_prof(ix, iy, box, 2, 2, 12, center=(0.0, 0.0), r=(1.0, 2.0, 4.0),
+                      fr=(0.0, 1.0, 0.5), dtype=np.float64)
+    rr = np.hypot(p[0] - 32.0, p[1] - 32.0) * dx
+    assert rr.min() >= 1.0 - 1e-12 and rr.max() <= 4.0 + 1e-12
+    assert np.allclose(p[7], -0.25 * np.interp(rr, [1.0, 2.0, 4.0], [0.0, 1.0, 0.5]), atol=1e-12)
+    p = O.dist2d_prof(ix, iy, box, 2, 2, 0, s=5.0, long_s=(0.0, 10.0), long_fs=(1.0, 3.0),
+                      dtype=np.float64)
+    assert np.allclose(p[7], -0.25 * 2.0)
+
+
 def _oracle_fields(O, cfg, nslices):
     s = O.Sim(cfg, np.float64)
     s.begin3d()
