@@ -167,7 +167,8 @@ def make_engine(qpgpu, cfg, device):
                                   peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                   center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
     sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False,
-                           dt=cfg.get("dt", 0.0), tol=cfg.get("tol", 0.0))
+                           dt=cfg.get("dt", 0.0), tol=cfg.get("tol", 0.0),
+                           predict=cfg.get("predict", False))
     return ctx, sp, beams, sim
 
 

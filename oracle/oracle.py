@@ -293,7 +293,7 @@ def beam_push(part, fxyz, bxyz, qbm, dt, dex, dxi, ind3, dtype=np.float32):
 
 
 # -------------------------------------------------------------- simulation
-P_FIXED = 21
+P_FIXED = 22
 B_NPAR = 18
 W = dict(psi=1, fxy=2, bxyz=3, psit=4, cu=5, dcu=6, amu=7, epw_k=8, cu_k=9, qe=10, qb=11,
          epwb_k=12, ppart=13, kpic=14, bexyz=15, bbxyz=16, q3=17, q3d=18, qn=19, beam0=20,
@@ -319,6 +319,7 @@ def sim_params(cfg) -> np.ndarray:
     p[18] = cfg.get("dt", 0.0)  # 3D time step; > 0 pushes the beams after the slices
     p[19] = cfg.get("tol", 0.0)  # > 0: B passes per slice until |d epw| <= tol |epw|
     p[20] = 1 if cfg.get("vpot", False) else 0  # keep the 3D vector potential
+    p[21] = 1 if cfg.get("predict", False) else 0  # start B from 2 epw(j-1) - epw(j-2)
     for b, bm in enumerate(cfg["beams"]):
         o = P_FIXED + B_NPAR * b
         p[o:o + 3] = bm["np"]

@@ -80,7 +80,17 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
     const float psit = QM(k_pot(K, kx, ky, k_div(K, kx, ky, cx, cy)), -a.dex);
     float bx, by, bz;
     k_bf(K, kx, ky, cx, cy, cz, &bx, &by, &bz);
-    k_assemble_mode(a.epw_x[o], a.epw_y[o], ebx, eby, a.dex, &bx, &by, &bz);
+    float ex = a.epw_x[o], ey = a.epw_y[o];
+    if (a.epw_prev_x) {
+      const float ex1 = ex, ey1 = ey;
+      ex = QS(QM(2.f, ex1), a.epw_prev_x[o]);
+      ey = QS(QM(2.f, ey1), a.epw_prev_y[o]);
+      a.epw_x[o] = ex;
+      a.epw_y[o] = ey;
+      a.epw_prev_x[o] = ex1;
+      a.epw_prev_y[o] = ey1;
+    }
+    k_assemble_mode(ex, ey, ebx, eby, a.dex, &bx, &by, &bz);
     line[0][ky] = bz;
     line[2][ky] = psi;
     line[3][ky] = fx;

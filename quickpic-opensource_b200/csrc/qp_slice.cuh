@@ -13,7 +13,10 @@ struct SliceA {
   const float* qe;
   const float* qb;  // null without beams
   const float *cu_x, *cu_y, *cu_z;
-  const float *epw_x, *epw_y;
+  float *epw_x, *epw_y;
+  // optional predictor: B_perp two slices back; with it epw becomes
+  // 2 epw - epw_prev (written back) and epw_prev takes the old epw
+  float *epw_prev_x, *epw_prev_y;
   float *epwb_x, *epwb_y;
   float *out_psi, *out_fx, *out_fy, *out_psit, *out_bx, *out_by, *out_bz;
   float norm, dex;

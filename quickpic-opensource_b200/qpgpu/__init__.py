@@ -101,7 +101,7 @@ class _BeamDesc(C.Structure):
 class _SimDesc(C.Structure):
     _fields_ = [("iter", C.c_int), ("store3d", C.c_int), ("use_graphs", C.c_int),
                 ("dt", C.c_float), ("tol", C.c_float), ("vpot", C.c_int),
-                ("reserved", C.c_int * 2)]
+                ("predict", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class StepStats(C.Structure):
@@ -439,11 +439,12 @@ class Simulation:
     """The fused 3D step: beam deposit, every slice, species renew, on the GPU."""
 
     def __init__(self, ctx: Context, species, beams, iter=2, store3d=True, use_graphs=False,
-                 dt=0.0, tol=0.0, vpot=False):
+                 dt=0.0, tol=0.0, vpot=False, predict=False):
         d = _SimDesc()
         d.iter = iter  # passes per slice; with tol > 0 the most passes a slice may take
         d.tol = tol  # > 0: stop a slice's passes once |d epw| / |epw| <= tol
         d.vpot = 1 if vpot else 0  # keep the 3D vector potential ("vpot")
+        d.predict = 1 if predict else 0  # start B from 2 epw(j-1) - epw(j-2)
         d.store3d = 1 if store3d else 0
         d.use_graphs = 1 if use_graphs else 0
         d.dt = dt  # 3D time step; > 0 ends every step with the beam push

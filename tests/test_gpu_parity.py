@@ -375,7 +375,8 @@ def _gpu_sim(qp, cfg, use_graphs=False, dt=0.0):
                                peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
     sim = qp.Simulation(c, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=use_graphs,
-                        dt=dt, tol=cfg.get("tol", 0.0), vpot=cfg.get("vpot", False))
+                        dt=dt, tol=cfg.get("tol", 0.0), vpot=cfg.get("vpot", False),
+                        predict=cfg.get("predict", False))
     return c, sp, beams, sim
 
 
@@ -427,14 +428,17 @@ def test_full_3d_step_matches_oracle(qp, oracle_mod, use_graphs=False):
     c.close()
 
 
-def test_convergence_controlled_step_matches_oracle(qp, oracle_mod):
+@pytest.mark.parametrize("predict", [False, True], ids=["carry", "extrapolate"])
+def test_convergence_controlled_step_matches_oracle(qp, oracle_mod, predict):
     """B passes stop per slice once |d epw| <= 1e-4 |epw| (at most 12), decided on
     the device.  The pass count follows the FP64 oracle's (the FP32 residual may
     cross the tolerance one pass earlier or later in a few slices) and the
-    converged fields match it."""
+    converged fields match it; likewise when each slice starts from the linear
+    extrapolation of the two previous slices' B_perp."""
     O = oracle_mod
     cfg = make_config(ind=(6, 6, 5), iter=12)
     cfg["tol"] = 1e-4
+    cfg["predict"] = predict
     c, sp, beams, sim = _gpu_sim(qp, cfg)
     st = sim.step3d()
     o64 = O.Sim(cfg, np.float64)
