@@ -48,6 +48,15 @@ CONFIGS = {
                                peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                                sigma=[0.3, 0.3, 0.6],
                                sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the medium case, B to 1e-4, each slice's B passes started from the quadratic
+    # extrapolation of the three previous slices' B_perp (the predictor form)
+    "medium_predict": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=16, tol=1e-4, predict=2,
+                           dt=10.0,
+                           species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                           beams=[dict(np=[256, 256, 128], q=-1.0, m=1.0, gamma=20000.0,
+                                       peak_density=4.0, quiet_start=True,
+                                       center=[0.0, 0.0, 3.0], sigma=[0.3, 0.3, 0.6],
+                                       sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the medium case with the reference's fixed 2 B passes per slice (no tolerance)
     "medium_fixed2": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2, dt=10.0,
                           species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
@@ -415,9 +424,11 @@ def workload_desc(cfg, name):
 
 
 def passes_desc(cfg):
+    start = {1: ", started from the linear extrapolation of B_perp",
+             2: ", started from the quadratic extrapolation of B_perp"}.get(cfg.get("predict", 0), "")
     if cfg.get("tol", 0.0) > 0:
         return (f"B predictor-corrector passes per slice until the relative change of B_perp "
-                f"<= {cfg['tol']:g} (at most {cfg['iter']})")
+                f"<= {cfg['tol']:g} (at most {cfg['iter']}){start}")
     return f"iter={cfg['iter']} (fixed predictor-corrector passes)"
 
 

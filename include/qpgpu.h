@@ -266,9 +266,10 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * actually run are returned in qp_step_stats.iterations);
  * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
  * predict = 1 starts each slice's B passes from the linear extrapolation
- * 2 epw(j-1) - epw(j-2) of the transverse B of the two previous slices
- * instead of epw(j-1) (the reference's start); with tol > 0 the passes still
- * run to the same tolerance;
+ * 2 epw(j-1) - epw(j-2) of the transverse B of the two previous slices,
+ * predict = 2 from the quadratic 3 epw(j-1) - 3 epw(j-2) + epw(j-3), instead
+ * of epw(j-1) (the reference's start); with tol > 0 the passes still run to
+ * the same tolerance;
  * vpot = 1 (with store3d = 1, one species) also keeps the vector potential
  * vpot3d of every slice (simulation_class.f03:711-716: field2d%vpot of the
  * last pass's current, fftkr, times -dex), downloaded as "vpot";

@@ -319,7 +319,7 @@ def sim_params(cfg) -> np.ndarray:
     p[18] = cfg.get("dt", 0.0)  # 3D time step; > 0 pushes the beams after the slices
     p[19] = cfg.get("tol", 0.0)  # > 0: B passes per slice until |d epw| <= tol |epw|
     p[20] = 1 if cfg.get("vpot", False) else 0  # keep the 3D vector potential
-    p[21] = 1 if cfg.get("predict", False) else 0  # start B from 2 epw(j-1) - epw(j-2)
+    p[21] = int(cfg.get("predict", 0))  # B start: 1 linear, 2 quadratic extrapolation
     for b, bm in enumerate(cfg["beams"]):
         o = P_FIXED + B_NPAR * b
         p[o:o + 3] = bm["np"]

@@ -83,8 +83,16 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
     float ex = a.epw_x[o], ey = a.epw_y[o];
     if (a.epw_prev_x) {
       const float ex1 = ex, ey1 = ey;
-      ex = QS(QM(2.f, ex1), a.epw_prev_x[o]);
-      ey = QS(QM(2.f, ey1), a.epw_prev_y[o]);
+      const float ex0 = a.epw_prev_x[o], ey0 = a.epw_prev_y[o];
+      if (a.epw_prev2_x) {
+        ex = QA(QM(3.f, QS(ex1, ex0)), a.epw_prev2_x[o]);
+        ey = QA(QM(3.f, QS(ey1, ey0)), a.epw_prev2_y[o]);
+        a.epw_prev2_x[o] = ex0;
+        a.epw_prev2_y[o] = ey0;
+      } else {
+        ex = QS(QM(2.f, ex1), ex0);
+        ey = QS(QM(2.f, ey1), ey0);
+      }
       a.epw_x[o] = ex;
       a.epw_y[o] = ey;
       a.epw_prev_x[o] = ex1;

@@ -14,9 +14,11 @@ struct SliceA {
   const float* qb;  // null without beams
   const float *cu_x, *cu_y, *cu_z;
   float *epw_x, *epw_y;
-  // optional predictor: B_perp two slices back; with it epw becomes
-  // 2 epw - epw_prev (written back) and epw_prev takes the old epw
+  // optional predictor: B_perp two (and three) slices back; epw becomes
+  // 2 epw - epw_prev, or 3 epw - 3 epw_prev + epw_prev2 (written back), and the
+  // history shifts by one slice
   float *epw_prev_x, *epw_prev_y;
+  float *epw_prev2_x, *epw_prev2_y;  // quadratic predictor only
   float *epwb_x, *epwb_y;
   float *out_psi, *out_fx, *out_fy, *out_psit, *out_bx, *out_by, *out_bz;
   float norm, dex;

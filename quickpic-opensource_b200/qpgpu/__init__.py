@@ -444,7 +444,8 @@ class Simulation:
         d.iter = iter  # passes per slice; with tol > 0 the most passes a slice may take
         d.tol = tol  # > 0: stop a slice's passes once |d epw| / |epw| <= tol
         d.vpot = 1 if vpot else 0  # keep the 3D vector potential ("vpot")
-        d.predict = 1 if predict else 0  # start B from 2 epw(j-1) - epw(j-2)
+        # start B from 2 epw(j-1) - epw(j-2) (True or 1) or 3 epw(j-1) - 3 epw(j-2) + epw(j-3) (2)
+        d.predict = int(predict)
         d.store3d = 1 if store3d else 0
         d.use_graphs = 1 if use_graphs else 0
         d.dt = dt  # 3D time step; > 0 ends every step with the beam push

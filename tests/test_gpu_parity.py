@@ -428,7 +428,7 @@ def test_full_3d_step_matches_oracle(qp, oracle_mod, use_graphs=False):
     c.close()
 
 
-@pytest.mark.parametrize("predict", [False, True], ids=["carry", "extrapolate"])
+@pytest.mark.parametrize("predict", [0, 1, 2], ids=["carry", "linear", "quadratic"])
 def test_convergence_controlled_step_matches_oracle(qp, oracle_mod, predict):
     """B passes stop per slice once |d epw| <= 1e-4 |epw| (at most 12), decided on
     the device.  The pass count follows the FP64 oracle's (the FP32 residual may
