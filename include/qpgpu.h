@@ -223,11 +223,37 @@ int qp_species_download_q3(qp_species* sp, int pos, float* rf);
 
 /* --------------------------------------------------------------- beam3d */
 
-/* Tri-Gaussian beam, profile 0 (fdist3d_000, fdist3d_class.f03:222-421) with
- * the keys beam(i).{np, q, m, gamma, peak_density, quiet_start, center, sigma,
- * sigma_v, npmax}; loaded with PRVDIST32_RANDOM and ranorm's fixed seeds
- * (part3d_lib77.f:411-552, 1324-1383).  Beams created on one context draw
- * from one ranorm sequence, in creation order, like the reference. */
+/* A beam3d and its fdist3d profile (fdist3d_class.f03), with the keys of
+ * beam(i) in the input file.  Lengths are in the box's units, like the input.
+ * Beams created on one context draw from one ranorm sequence, in creation
+ * order, like the reference.
+ *  profile 0 (fdist3d_000, 222-421): tri-Gaussian by PRVDIST32_RANDOM
+ *    (part3d_lib77.f:411-552) with ranorm's fixed seeds (1324-1383): np,
+ *    q, m, gamma, peak_density, quiet_start, center, sigma, sigma_v, npmax,
+ *    centroid_x, centroid_y, static_density;
+ *  profile 1 (fdist3d_001, 423-650): Gaussian in x, y and the piecewise
+ *    profile fz(z) in z by PRVDIST32_RAN_PFL (part3d_lib77.f:193-410): as
+ *    profile 0 without sigma[2], plus piecewise_z/fz (npiece points, z
+ *    increasing).  Its longitudinal acceptance draws use RANDOM_NUMBER in the
+ *    reference, a compiler runtime's generator; here SplitMix64 from `seed`;
+ *  profile 2 (fdist3d_002, 652-821): Twiss beam by PRVDIST32_TWISS
+ *    (part3d_lib77.f:1-191): np, q, m, gamma, peak_density, quiet_start,
+ *    center, alpha, beta, emittance, sigma[2] = sigmaz, sigma_v[2] =
+ *    sigma_vz, npmax;
+ *  profile 3 (fdist3d_003, 823-974): np[0] particles read from the text
+ *    file file_name, one "z x y pz px py q" per line, positions in
+ *    micrometres (divided by c/omega_p = 5.32150254e9 / sqrt(n0) um, n0 the
+ *    plasma density in cm^-3; z measured backwards from the box front; x, y
+ *    from center), momenta and charge as they are; particles outside the box
+ *    are left out;
+ *  profile 100 (fdist3d_100, 976-1166): ring of radius r1 and width r2 about
+ *    center, ppc particles per cell in the box range_x/y/z, weights q/|q|
+ *    peak_density exp(-(dz^2 + (r - r1)^2) / (2 r2^2)) / (ppc product), pz =
+ *    gamma.
+ * static_density = 1 (beam(i).static, profiles 0 and 1) puts the profile's
+ * analytic density on the 3D grid and loads no particles: no deposit, no
+ * push.  frozen = 1 is beam(i).evolution = false: the push leaves the beam
+ * where it is (push_beam3d, beam3d_class.f03:169-172). */
 typedef struct {
   int profile;
   int np[3];
@@ -235,6 +261,18 @@ typedef struct {
   int quiet_start;
   float center[3], sigma[3], sigma_v[3];
   long long npmax;
+  float centroid_x[3], centroid_y[3];
+  int static_density, frozen, npiece;
+  int ppc[3];
+  const float* piecewise_z;
+  const float* piecewise_fz;
+  const char* file_name;
+  unsigned long long seed;
+  float alpha[2], beta[2], emittance[2];
+  float n0;
+  float range_x[2], range_y[2], range_z[2];
+  float r1, r2;
+  float reserved[1];
 } qp_beam_desc;
 
 int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out);

@@ -257,21 +257,114 @@ def beam_qm(q, peak, sig, lo, hi, indx, indy, indz, npx, npy, npz, dtype=np.floa
 
 
 def beam_load(qm, sigv, gamma, np3, ind3, sig_cells, center_cells, quiet=True,
-              npmax=None, dtype=np.float32):
-    """PRVDIST32_RANDOM from the fixed ranorm seeds (caller resets ranorm)."""
+              npmax=None, cx=(0, 0, 0), cy=(0, 0, 0), dtype=np.float32):
+    """PRVDIST32_RANDOM from the fixed ranorm seeds (caller resets ranorm); cx, cy
+    are the centroid polynomials in cells."""
     npx, npy, npz = np3
     if npmax is None:
         npmax = npx * npy * npz + 2
     part = np.zeros((7, npmax), dtype=dtype, order="F")
     npp = C.c_int(0)
-    z3 = np.zeros(3, dtype=dtype)
     rc = _call("oq_prvdist32_random", dtype, part, npmax, C.byref(npp), float(qm),
                float(sigv[0]), float(sigv[1]), float(sigv[2]), float(gamma), npx, npy, npz,
                ind3[0], ind3[1], ind3[2], float(sig_cells[0]), float(sig_cells[1]),
                float(sig_cells[2]), float(center_cells[0]), float(center_cells[1]),
-               float(center_cells[2]), z3, z3, 1 if quiet else 0)
+               float(center_cells[2]), np.asarray(cx, dtype=dtype),
+               np.asarray(cy, dtype=dtype), 1 if quiet else 0)
     assert rc == 0, rc
     return part[:, : npp.value].copy(order="F")
+
+
+def dist3d_001_zf(z, fz, zmin, dz, nz, dtype=np.float32):
+    """init_fdist3d_001's sumz and dist3d_001's slice table zf(1:nz)."""
+    zz = np.ascontiguousarray(z, dtype=dtype)
+    ff = np.ascontiguousarray(fz, dtype=dtype)
+    zf = np.zeros(nz, dtype=dtype)
+    sumz = np.zeros(1, dtype=dtype)
+    rc = _call("oq_dist3d_001_zf", dtype, zz, ff, zz.size, float(zmin), float(dz), nz, zf, sumz)
+    assert rc == 0, "piecewise_z is not increasing"
+    return zf, float(sumz[0])
+
+
+def beam_qm2(q, peak, e, sx, sy, sz, dx, dy, dz, npx, npy, npz, dtype=np.float32):
+    """Charge per particle of beam profiles 1 (e = 1, sz = sumz) and 2 (e = 1.5)."""
+    out = np.zeros(1, dtype=dtype)
+    _call("oq_beam_qm2", dtype, float(q), float(peak), float(e), float(sx), float(sy), float(sz),
+          float(dx), float(dy), float(dz), npx, npy, npz, out)
+    return float(out[0])
+
+
+def beam_load_pfl(qm, center_cells, sig_cells, sigv, gamma, cx, cy, np3, n3, dp, quiet=True,
+                  seed=0x5eed, npmax=None, dtype=np.float32):
+    """PRVDIST32_RAN_PFL (caller resets ranorm); dp = the slice profile zf(1:nz)."""
+    npx, npy, npz = np3
+    if npmax is None:
+        npmax = npx * npy * npz + 8
+    part = np.zeros((7, npmax), dtype=dtype, order="F")
+    npp = C.c_int(0)
+    d = np.array(dp, dtype=dtype)
+    rc = _call("oq_prvdist32_ran_pfl", dtype, part, npmax, C.byref(npp), float(qm),
+               float(center_cells[0]), float(center_cells[1]), float(center_cells[2]),
+               float(sig_cells[0]), float(sig_cells[1]), float(sigv[0]), float(sigv[1]),
+               float(sigv[2]), float(gamma), np.asarray(cx, dtype=dtype),
+               np.asarray(cy, dtype=dtype), npx, npy, npz, n3[0], n3[1], n3[2], d,
+               1 if quiet else 0, C.c_ulonglong(seed))
+    assert rc == 0, rc
+    return part[:, : npp.value].copy(order="F")
+
+
+def beam_load_twiss(qm, alpha, beta_cells, emit_cells, sigz_cells, sigvz, gamma, np3, n3,
+                    center_cells, quiet=True, npmax=None, dtype=np.float32):
+    """PRVDIST32_TWISS (caller resets ranorm)."""
+    npx, npy, npz = np3
+    if npmax is None:
+        npmax = npx * npy * npz + 8
+    part = np.zeros((7, npmax), dtype=dtype, order="F")
+    npp = C.c_int(0)
+    rc = _call("oq_prvdist32_twiss", dtype, part, npmax, C.byref(npp), float(qm),
+               np.asarray(alpha, dtype=dtype), np.asarray(beta_cells, dtype=dtype),
+               np.asarray(emit_cells, dtype=dtype), float(sigz_cells), float(gamma),
+               float(sigvz), npx, npy, npz, n3[0], n3[1], n3[2], float(center_cells[0]),
+               float(center_cells[1]), float(center_cells[2]), 1 if quiet else 0)
+    assert rc == 0, rc
+    return part[:, : npp.value].copy(order="F")
+
+
+def beam_load_file(path, npt, x0, y0, dx, dy, dz, cwp, n3, npmax=None, dtype=np.float32):
+    """dist3d_003: particles read from a text file."""
+    if npmax is None:
+        npmax = max(npt, 1)
+    part = np.zeros((7, npmax), dtype=dtype, order="F")
+    npp = C.c_int(0)
+    rc = _call("oq_dist3d_003", dtype, str(path).encode(), npt, part, npmax, C.byref(npp),
+               float(x0), float(y0), float(dx), float(dy), float(dz), float(cwp), n3[0], n3[1],
+               n3[2])
+    assert rc == 0, rc
+    return part[:, : npp.value].copy(order="F")
+
+
+def beam_load_ring(ppc, qm, amp, gamma, bc, lb, ub, r1, r2, n3, npmax, dtype=np.float32):
+    """dist3d_100: a ring on a lattice of ppc particles per cell."""
+    part = np.zeros((7, npmax), dtype=dtype, order="F")
+    npp = C.c_int(0)
+    rc = _call("oq_dist3d_100", dtype, part, npmax, C.byref(npp),
+               np.asarray(ppc, dtype=np.int32), float(qm), float(amp), float(gamma),
+               np.asarray(bc, dtype=dtype), np.asarray(lb, dtype=dtype),
+               np.asarray(ub, dtype=dtype), float(r1), float(r2), n3[0], n3[1], n3[2])
+    assert rc == 0, rc
+    return part[:, : npp.value].copy(order="F")
+
+
+def beam_static(amp, center_cells, sig_cells, cx, cy, zf, n3, dtype=np.float32):
+    """Static-beam density of dist3d_000 (zf None) or dist3d_001 as q3(nx+2, ny+1, nz+1)."""
+    nx, ny, nz = n3
+    q3 = np.zeros((nx + 2, ny + 1, nz + 1), dtype=dtype, order="F")
+    zp = None if zf is None else np.ascontiguousarray(zf, dtype=dtype)
+    _call("oq_beam_static", dtype, float(amp), float(center_cells[0]), float(center_cells[1]),
+          float(center_cells[2]), float(sig_cells[0]), float(sig_cells[1]),
+          float(sig_cells[2]), np.asarray(cx, dtype=dtype), np.asarray(cy, dtype=dtype),
+          zp if zp is not None else C.c_void_p(0), nx, ny, nz, q3)
+    return q3
 
 
 def beam_deposit(part, ind3, dtype=np.float32):

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -1638,6 +1639,380 @@ int prvdist32_random(T* part, int npmax, int* npp, T qm, T vtx, T vty, T vtz, T 
   return ierr;
 }
 
+// Stand-in for the Fortran intrinsic RANDOM_NUMBER that PRVDIST32_RAN_PFL
+// calls (a compiler runtime's generator, which the reference does not pin):
+// SplitMix64 (Steele, Lea, Flood 2014) from a 64-bit seed, each number the
+// top 24 bits of an output times 2^-24.  The engine's loader defines the same.
+struct OUniform {
+  uint64_t s;
+  float next() {
+    s += 0x9e3779b97f4a7c15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z = z ^ (z >> 31);
+    return (float)(z >> 40) * (1.0f / 16777216.0f);
+  }
+};
+
+// init_fdist3d_001 fdist3d_class.f03:508-518 (sumz, the trapezoid integral
+// of fz over z, and the conversion z = (z - min) / dz) and the table of
+// dist3d_001 600-611: zf(i), i = 1..nz, linear between the points.
+template <class T>
+int dist3d_001_zf(const T* z, const T* fz, int nzf, T zmin, T dz, int nz, T* zf, T* sumz) {
+  T sum = T(0.0);
+  for (int ii = 2; ii <= nzf; ++ii) {
+    if (z[ii - 1] <= z[ii - 2]) return -1;  // "Piecewise_z is not monotonically increasing"
+    sum = sum + (fz[ii - 1] + fz[ii - 2]) * (z[ii - 1] - z[ii - 2]) * T(0.5);
+  }
+  *sumz = sum;
+  std::vector<T> zz(nzf);
+  for (int ii = 1; ii <= nzf; ++ii) zz[ii - 1] = (z[ii - 1] - zmin) / dz;
+  for (int i = 1; i <= nz; ++i) {
+    zf[i - 1] = T(0.0);
+    for (int j = 2; j <= nzf; ++j) {
+      if (((T)i >= zz[j - 2]) && ((T)i < zz[j - 1])) {
+        zf[i - 1] = fz[j - 1] + (fz[j - 2] - fz[j - 1]) / (zz[j - 2] - zz[j - 1]) * ((T)i - zz[j - 1]);
+        break;
+      }
+    }
+  }
+  return 0;
+}
+
+// init_fdist3d_001 521-526 (e = 1, sz = sumz) and init_fdist3d_002 732-737
+// (e = 1.5, sz = sigz): the charge of one macro-particle.
+template <class T>
+T beam_qm2(T qm, T np, T e, T sx, T sy, T sz, T dx, T dy, T dz, int npx, int npy, int npz) {
+  const T twopi = T(2) * (T)3.1415926535897932f;
+  qm = qm / std::abs(qm) * std::abs(np) * (e == T(1) ? twopi : (T)std::pow(twopi, e)) * sx * sy *
+       sz;
+  qm = qm / dx / dy / dz;
+  qm = qm / (T)npx;
+  qm = qm / (T)npy;
+  qm = qm / (T)npz;
+  return qm;
+}
+
+// PRVDIST32_RAN_PFL, part3d_lib77.f:193-410, one partition (edges 0, ny,
+// 0, nz).  dp(nz) is the longitudinal profile and is rescaled in place as in
+// the reference.  The reference stores while npt <= npmax, which lets npp
+// reach npmax + 1, one past its array; here a particle is stored only while
+// npp < npmax and each refused one counts in ierr.  An all-zero profile
+// returns no particles (the reference would draw forever).
+template <class T>
+int prvdist32_ran_pfl(T* part, int npmax, int* npp, T qm, T x0, T y0, T z0, T sigx, T sigy,
+                      T vtx, T vty, T vtz, T vdx, T vdy, T vdz, const T* cx, const T* cy, int npx,
+                      int npy, int npz, int nx, int ny, int nz, T* dp, bool lquiet,
+                      uint64_t seed) {
+  int ierr = 0;
+  (void)vdx;
+  (void)vdy;
+  const T edges[4] = {T(0), T(ny), T(0), T(nz)};
+  int npt = 1;
+  const T x2 = T(2.0) * x0, y2 = T(2.0) * y0;
+  const T borderlx = std::max(x0 - T(5.0) * sigx, T(1.0));
+  const T borderly = std::max(y0 - T(5.0) * sigy, T(1.0));
+  const T borderx = std::min(x0 + T(5.0) * sigx, T(nx - 1));
+  const T bordery = std::min(y0 + T(5.0) * sigy, T(ny - 1));
+  const int nz1 = nz - 1;
+  T amax = T(0);
+  for (int i = 1; i <= nz; ++i) {
+    dp[i - 1] = std::abs(dp[i - 1]);
+    amax = std::max(amax, dp[i - 1]);
+  }
+  *npp = 0;
+  if (!(amax > T(0)) || nz1 < 1) return 0;
+  amax = amax * (T)1.2f;
+  for (int i = 1; i <= nz; ++i) dp[i - 1] = dp[i - 1] / amax;
+  OUniform uni{seed};
+  T tmpu[1024], tmpz[1024];
+  int cnt = 0;
+  int j = 0, l = npz;
+  while (j < npx) {
+    int k = 0;
+    while (k < npy) {
+      l = l - npz;
+      while (l < npz) {
+        if (cnt <= 0) {  // call RANDOM_NUMBER(tmpu); call RANDOM_NUMBER(tmpz)
+          for (int i = 0; i < 1024; ++i) tmpu[i] = (T)uni.next();
+          for (int i = 0; i < 1024; ++i) tmpz[i] = (T)uni.next();
+          cnt = 1024;
+        }
+        const T u = tmpu[cnt - 1];
+        const T tempz = tmpz[cnt - 1] * (T)nz1;
+        cnt = cnt - 1;
+        int zi = (int)tempz;
+        if (zi > nz1 - 1) zi = nz1 - 1;
+        const T zf = tempz - (T)zi;
+        const T zs = T(1.) - zf;
+        zi = zi + 1;
+        const T dpi = dp[zi - 1] * zs + dp[zi] * zf;
+        if (u <= dpi) {
+          T tempx, tempy;
+          do {
+            tempx = (T)((double)x0 + (double)sigx * oq_ranorm());
+          } while (tempx >= borderx || tempx <= borderlx);
+          do {
+            tempy = (T)((double)y0 + (double)sigy * oq_ranorm());
+          } while (tempy >= bordery || tempy <= borderly);
+          if ((tempy < edges[1]) && (tempy > edges[0]) && (tempz < edges[3]) &&
+              (tempz > edges[2])) {
+            const T tvtx = (T)((double)vtx * oq_ranorm());
+            const T tvty = (T)((double)vty * oq_ranorm());
+            T tvtz = (T)((double)vtz * oq_ranorm() + (double)vdz);
+            tvtz = std::sqrt(tvtz * tvtz - T(1) - tvtx * tvtx - tvty * tvty);
+            T tempxx = T(0), tempyy = T(0);
+            if (npt <= npmax && *npp < npmax) {
+              npt = *npp + 1;
+              T* p = &part[7 * (size_t)(npt - 1)];
+              p[2] = tempz;
+              const T d = p[2] - z0;
+              tempxx = -(cx[0] * (d * d)) - cx[1] * d - cx[2];
+              p[0] = tempx + tempxx;
+              tempyy = -(cy[0] * (d * d)) - cy[1] * d - cy[2];
+              p[1] = tempy + tempyy;
+              p[3] = tvtx;
+              p[4] = tvty;
+              p[5] = tvtz;
+              p[6] = qm;
+              *npp = npt;
+            } else {
+              ierr = ierr + 1;
+            }
+            if (lquiet) {
+              if (npt <= npmax && *npp < npmax) {
+                npt = *npp + 1;
+                T* p = &part[7 * (size_t)(npt - 1)];
+                p[2] = tempz;
+                p[0] = x2 - tempx + tempxx;
+                p[1] = y2 - tempy + tempyy;
+                p[3] = -tvtx;
+                p[4] = -tvty;
+                p[5] = tvtz;
+                p[6] = qm;
+                *npp = npt;
+              } else {
+                ierr = ierr + 1;
+              }
+            }
+          }
+          l = l + 1;
+          if (lquiet) l = l + 1;
+        }
+      }
+      k = k + 1;
+    }
+    j = j + 1;
+  }
+  return ierr;
+}
+
+// PRVDIST32_TWISS, part3d_lib77.f:1-191, one partition.  tempx, tempy, tempz
+// and at1 are double precision in the reference, tx, ty and the velocities
+// real; the drift sums at its end are computed but never applied, and are
+// left out.  Storage as in prvdist32_ran_pfl (npt <= npmax, at most npmax).
+template <class T>
+int prvdist32_twiss(T* part, int npmax, int* npp, T qm, T alpha_x, T alpha_y, T beta_x,
+                    T beta_y, T emt_x, T emt_y, T sigz, T vdz, T vtz, int npx, int npy, int npz,
+                    int nx, int ny, int nz, T x0, T y0, T z0, T gamma, bool lquiet) {
+  int ierr = 0;
+  int npt = 1;
+  *npp = 0;
+  const T edges[4] = {T(0), T(ny), T(0), T(nz)};
+  const T x2 = T(2.0) * x0, y2 = T(2.0) * y0;
+  const T sigx = std::sqrt(beta_x * emt_x / gamma);
+  const T sigy = std::sqrt(beta_y * emt_y / gamma);
+  const T vtx = emt_x / sigx, vty = emt_y / sigy;
+  const T borderlx = std::max(x0 - T(3.0) * sigx, T(1.0));
+  const T borderly = std::max(y0 - T(3.0) * sigy, T(1.0));
+  const T borderlz = std::max(z0 - T(3.0) * sigz, T(1.0));
+  const T borderx = std::min(x0 + T(3.0) * sigx, T(nx - 1));
+  const T bordery = std::min(y0 + T(3.0) * sigy, T(ny - 1));
+  const T borderz = std::min(z0 + T(3.0) * sigz, T(nz - 1));
+  int j = 0, l = npz;
+  while (j < npx) {
+    int k = 0;
+    while (k < npy) {
+      l = l - npz;
+      while (l < npz) {
+        double tempz, tempx, tempy;
+        T tx, ty;
+      L10:
+        tempz = (double)z0 + (double)sigz * oq_ranorm();
+        if (tempz >= (double)borderz || tempz <= (double)borderlz) goto L10;
+      L20:
+        tx = (T)oq_ranorm();
+        tempx = (double)(x0 + sigx * tx);
+        if (tempx >= (double)borderx || tempx <= (double)borderlx) goto L20;
+      L30:
+        ty = (T)oq_ranorm();
+        tempy = (double)(y0 + sigy * ty);
+        if (tempy >= (double)bordery || tempy <= (double)borderly) goto L30;
+        if ((tx * tx + ty * ty) > T(9.0)) goto L20;
+        T tvtx = (T)((double)vtx * oq_ranorm());
+        T tvty = (T)((double)vty * oq_ranorm());
+        const T tvtz = (T)((double)vtz * oq_ranorm() + (double)vdz);
+        tvtx = (T)((double)tvtx - (double)(gamma * alpha_x / beta_x) * (tempx - (double)x0));
+        tvty = (T)((double)tvty - (double)(gamma * alpha_y / beta_y) * (tempy - (double)y0));
+        if ((tempy >= (double)edges[0]) && (tempy < (double)edges[1]) &&
+            (tempz >= (double)edges[2]) && (tempz < (double)edges[3])) {
+          if (npt <= npmax && *npp < npmax) {
+            npt = *npp + 1;
+            T* p = &part[7 * (size_t)(npt - 1)];
+            p[2] = (T)tempz;
+            p[0] = (T)tempx;
+            p[1] = (T)tempy;
+            p[3] = tvtx;
+            p[4] = tvty;
+            p[5] = tvtz;
+            p[6] = qm;
+            *npp = npt;
+          } else {
+            ierr = ierr + 1;
+          }
+          if (lquiet) {
+            if (npt <= npmax && *npp < npmax) {
+              npt = *npp + 1;
+              T* p = &part[7 * (size_t)(npt - 1)];
+              p[2] = (T)tempz;
+              p[0] = (T)((double)x2 - tempx);
+              p[1] = (T)((double)y2 - tempy);
+              p[3] = -tvtx;
+              p[4] = -tvty;
+              p[5] = tvtz;
+              p[6] = qm;
+              *npp = npt;
+            } else {
+              ierr = ierr + 1;
+            }
+          }
+        }
+        l = l + 1;
+        if (lquiet) l = l + 1;
+      }
+      k = k + 1;
+    }
+    j = j + 1;
+  }
+  return ierr;
+}
+
+// dist3d_003, fdist3d_class.f03:899-974: npt lines "z x y vz vx vy q" read
+// from a text file (blank-separated numbers), converted to cells and kept
+// when inside the box.  Returns -1 on a failed read, -2 past npmax.
+template <class T>
+int dist3d_003(const char* file, int npt, T* part, int npmax, int* npp, T x0, T y0, T dx, T dy,
+               T dz, T cwp, int nx, int ny, int nz) {
+  std::FILE* f = std::fopen(file, "r");
+  if (!f) return -1;
+  int nps = 1;
+  for (int i = 1; i <= npt; ++i) {
+    // a REAL read: each decimal rounded once to T
+    T v[7];
+    const char* fmt = sizeof(T) == sizeof(float) ? "%f %f %f %f %f %f %f"
+                                                 : "%lf %lf %lf %lf %lf %lf %lf";
+    if (std::fscanf(f, fmt, &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6]) != 7) {
+      std::fclose(f);
+      return -1;
+    }
+    T tempz = v[0], tempx = v[1], tempy = v[2];
+    const T tempvz = v[3], tempvx = v[4], tempvy = v[5], tempq = v[6];
+    tempx = tempx / cwp / dx + x0;
+    tempy = tempy / cwp / dy + y0;
+    tempz = -(tempz / cwp / dz);
+    if ((tempx >= T(1)) && tempx <= T(nx - 1) && (tempy >= T(0)) && (tempy < T(ny)) &&
+        (tempz >= T(0)) && (tempz < T(nz))) {
+      if (nps > npmax) {
+        std::fclose(f);
+        return -2;
+      }
+      T* p = &part[7 * (size_t)(nps - 1)];
+      p[0] = tempx;
+      p[3] = tempvx;
+      p[1] = tempy;
+      p[4] = tempvy;
+      p[2] = tempz;
+      p[5] = tempvz;
+      p[6] = tempq;
+      nps = nps + 1;
+    }
+  }
+  *npp = nps - 1;
+  std::fclose(f);
+  return 0;
+}
+
+// dist3d_100, fdist3d_class.f03:1081-1166, one partition (noff = 0, nd2p =
+// ny, nd3p = nz).  Returns -2 past npmax.
+template <class T>
+int dist3d_100(T* part, int npmax, int* npp, const int* ppc, T qm, T np, T gamma, const T* bc,
+               const T* lb_in, const T* ub_in, T r1, T r2, int nx, int ny, int nz) {
+  T lb[3], ub[3];
+  *npp = 0;
+  lb[0] = std::max(lb_in[0], T(0.0));
+  ub[0] = std::min(ub_in[0], (T)nx);
+  if (lb_in[1] > (T)ny || ub_in[1] < T(0)) return 0;
+  lb[1] = std::max(lb_in[1], T(0));
+  ub[1] = std::min(ub_in[1], (T)ny);
+  if (lb_in[2] > (T)nz || ub_in[2] < T(0)) return 0;
+  lb[2] = std::max(lb_in[2], T(0));
+  ub[2] = std::min(ub_in[2], (T)nz);
+  int nps = 1;
+  for (int i = (int)lb[0]; i <= (int)ub[0] - 1; ++i)
+    for (int j = (int)lb[1]; j <= (int)ub[1] - 1; ++j)
+      for (int k = (int)lb[2]; k <= (int)ub[2] - 1; ++k)
+        for (int ix = 0; ix <= ppc[0] - 1; ++ix)
+          for (int iy = 0; iy <= ppc[1] - 1; ++iy)
+            for (int iz = 0; iz <= ppc[2] - 1; ++iz) {
+              if (nps > npmax) return -2;
+              const T tx = ((T)ix + T(0.5)) / (T)ppc[0] + (T)i - T(1);
+              const T ty = ((T)iy + T(0.5)) / (T)ppc[1] + (T)j - T(1);
+              const T tz = ((T)iz + T(0.5)) / (T)ppc[2] + (T)k - T(1);
+              T* p = &part[7 * (size_t)(nps - 1)];
+              p[0] = tx;
+              p[1] = ty;
+              p[2] = tz;
+              p[3] = T(0.0);
+              p[4] = T(0.0);
+              p[5] = gamma;
+              const T a1 = std::abs(tz - bc[2]);
+              const T a2 = std::sqrt((tx - bc[0]) * (tx - bc[0]) + (ty - bc[1]) * (ty - bc[1]));
+              const T a3 = std::abs(a2 - r1);
+              const T a4 = a1 * a1 + a3 * a3;
+              p[6] = qm * np * std::exp(-(a4 / (r2 * r2) * T(0.5)));
+              nps = nps + 1;
+            }
+  *npp = nps - 1;
+  return 0;
+}
+
+// The static branch of dist3d_000 (fdist3d_class.f03:392-408) and dist3d_001
+// (613-630), one partition: q3(i, j, k) for i = 1..nx, j = 1..ny, k = 1..nz
+// of a (nx+2, ny+1, nz+1) array; zf = null takes the Gaussian in z of 000.
+template <class T>
+void beam_static(T np, T x0, T y0, T z0, T sigx, T sigy, T sigz, const T* cx, const T* cy,
+                 const T* zf, int nx, int ny, int nz, T* q3) {
+  const size_t nxv = (size_t)nx + 2, nyv = (size_t)ny + 1;
+  for (int k = 1; k <= nz; ++k) {
+    const T zval = (T)(k - 1) - z0;
+    const T cx0 = -(cx[0] * (zval * zval)) - cx[1] * zval - cx[2];
+    const T cy0 = -(cy[0] * (zval * zval)) - cy[1] * zval - cy[2];
+    const T t1 = zf ? np * zf[k - 1] : np * std::exp(-(zval * zval / T(2.0) / (sigz * sigz)));
+    for (int i = 1; i <= nx; ++i) {
+      const T xval = (T)(i - 1);
+      const T dx = xval - x0 + cx0;
+      const T t2 = t1 * std::exp(-(dx * dx / T(2.0) / (sigx * sigx)));
+      for (int j = 1; j <= ny; ++j) {
+        const T yval = (T)(j - 1);
+        const T dy = yval - y0 + cy0;
+        q3[(size_t)(i - 1) + nxv * ((size_t)(j - 1) + nyv * (size_t)(k - 1))] =
+            t2 * std::exp(-(dy * dy / T(2.0) / (sigy * sigy)));
+      }
+    }
+  }
+}
+
 // PGBPUSH32L_QP, part3d_lib77.f:630-786 (one partition, noff = 0): the
 // quasi-static beam push with the 3D fields of the step.  fxyz and bxyz are
 // (3, nxv, nypmx, nzpmx); only the first two components of bxyz are used.
@@ -1895,6 +2270,49 @@ void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
     return prvdist32_random<T>(part, npmax, npp, qm, vtx, vty, vtz, T(0), T(0), vdz,    \
                                npx, npy, npz, 1 << indx, 1 << indy, 1 << indz, sigx,    \
                                sigy, sigz, x0, y0, z0, cx, cy, quiet != 0);             \
+  }                                                                                     \
+  extern "C" int oq_dist3d_001_zf_##S(const T* z, const T* fz, int nzf, T zmin, T dz,   \
+                                     int nz, T* zf, T* sumz) {                          \
+    return dist3d_001_zf<T>(z, fz, nzf, zmin, dz, nz, zf, sumz);                        \
+  }                                                                                     \
+  extern "C" int oq_beam_qm2_##S(T q, T np, T e, T sx, T sy, T sz, T dx, T dy, T dz,    \
+                                 int npx, int npy, int npz, T* qm_out) {                \
+    *qm_out = beam_qm2<T>(q, np, e, sx, sy, sz, dx, dy, dz, npx, npy, npz);             \
+    return 0;                                                                           \
+  }                                                                                     \
+  extern "C" int oq_prvdist32_ran_pfl_##S(                                              \
+      T* part, int npmax, int* npp, T qm, T x0, T y0, T z0, T sigx, T sigy, T vtx, T vty, \
+      T vtz, T vdz, const T* cx, const T* cy, int npx, int npy, int npz, int nx, int ny, \
+      int nz, T* dp, int quiet, unsigned long long seed) {                              \
+    return prvdist32_ran_pfl<T>(part, npmax, npp, qm, x0, y0, z0, sigx, sigy, vtx, vty, \
+                                vtz, T(0), T(0), vdz, cx, cy, npx, npy, npz, nx, ny, nz, \
+                                dp, quiet != 0, seed);                                  \
+  }                                                                                     \
+  extern "C" int oq_prvdist32_twiss_##S(                                                \
+      T* part, int npmax, int* npp, T qm, const T* alpha, const T* beta, const T* emt,  \
+      T sigz, T vdz, T vtz, int npx, int npy, int npz, int nx, int ny, int nz, T x0,    \
+      T y0, T z0, int quiet) {                                                          \
+    return prvdist32_twiss<T>(part, npmax, npp, qm, alpha[0], alpha[1], beta[0],        \
+                              beta[1], emt[0], emt[1], sigz, vdz, vtz, npx, npy, npz,   \
+                              nx, ny, nz, x0, y0, z0, vdz, quiet != 0);                 \
+  }                                                                                     \
+  extern "C" int oq_dist3d_003_##S(const char* file, int npt, T* part, int npmax,       \
+                                   int* npp, T x0, T y0, T dx, T dy, T dz, T cwp,       \
+                                   int nx, int ny, int nz) {                            \
+    return dist3d_003<T>(file, npt, part, npmax, npp, x0, y0, dx, dy, dz, cwp, nx, ny,  \
+                         nz);                                                           \
+  }                                                                                     \
+  extern "C" int oq_dist3d_100_##S(T* part, int npmax, int* npp, const int* ppc, T qm,  \
+                                   T np, T gamma, const T* bc, const T* lb,             \
+                                   const T* ub, T r1, T r2, int nx, int ny, int nz) {   \
+    return dist3d_100<T>(part, npmax, npp, ppc, qm, np, gamma, bc, lb, ub, r1, r2, nx,  \
+                         ny, nz);                                                       \
+  }                                                                                     \
+  extern "C" int oq_beam_static_##S(T np, T x0, T y0, T z0, T sigx, T sigy, T sigz,    \
+                                    const T* cx, const T* cy, const T* zf, int nx,      \
+                                    int ny, int nz, T* q3) {                            \
+    beam_static<T>(np, x0, y0, z0, sigx, sigy, sigz, cx, cy, zf, nx, ny, nz, q3);       \
+    return 0;                                                                           \
   }                                                                                     \
   extern "C" int oq_pgbpush32l_qp_##S(T* part, int npp, const T* fxyz, const T* bxyz,  \
                                       T qbm, T dt, T dex, T dxi, int indx, int indy,    \

@@ -88,6 +88,28 @@ extern "C" {
                               T vtz, T vdz, int npx, int npy, int npz, int indx,    \
                               int indy, int indz, T sigx, T sigy, T sigz, T x0,     \
                               T y0, T z0, const T* cx, const T* cy, int quiet);     \
+  /* beam profiles 1, 2, 3, 100 and static densities (fdist3d_class.f03) */        \
+  int oq_dist3d_001_zf_##S(const T* z, const T* fz, int nzf, T zmin, T dz, int nz,   \
+                           T* zf, T* sumz);                                          \
+  int oq_beam_qm2_##S(T q, T np, T e, T sx, T sy, T sz, T dx, T dy, T dz, int npx,  \
+                      int npy, int npz, T* qm_out);                                  \
+  int oq_prvdist32_ran_pfl_##S(T* part, int npmax, int* npp, T qm, T x0, T y0, T z0,\
+                               T sigx, T sigy, T vtx, T vty, T vtz, T vdz,          \
+                               const T* cx, const T* cy, int npx, int npy, int npz, \
+                               int nx, int ny, int nz, T* dp, int quiet,            \
+                               unsigned long long seed);                             \
+  int oq_prvdist32_twiss_##S(T* part, int npmax, int* npp, T qm, const T* alpha,    \
+                             const T* beta, const T* emt, T sigz, T vdz, T vtz,     \
+                             int npx, int npy, int npz, int nx, int ny, int nz,     \
+                             T x0, T y0, T z0, int quiet);                           \
+  int oq_dist3d_003_##S(const char* file, int npt, T* part, int npmax, int* npp,    \
+                        T x0, T y0, T dx, T dy, T dz, T cwp, int nx, int ny, int nz);\
+  int oq_dist3d_100_##S(T* part, int npmax, int* npp, const int* ppc, T qm, T np,   \
+                        T gamma, const T* bc, const T* lb, const T* ub, T r1, T r2, \
+                        int nx, int ny, int nz);                                     \
+  int oq_beam_static_##S(T np, T x0, T y0, T z0, T sigx, T sigy, T sigz,            \
+                         const T* cx, const T* cy, const T* zf, int nx, int ny,     \
+                         int nz, T* q3);                                             \
   int oq_pgpost32l_##S(const T* part, int npp, T* q3, int indx, int indy, int indz);\
   /* beam push PGBPUSH32L_QP with the 3D fields (3, nx+2, ny+1, nz+1); conducting  \
      boundaries drop particles; returns the new count */                             \

@@ -103,6 +103,8 @@ struct qp_beam {
   float qbm = 0.f;       // charge-to-mass ratio q/m of the push
   long long cap = 0;     // particle slots of each plane (the count at creation)
   int* keep = nullptr;   // per-particle flags of the push (allocated by the first push)
+  bool is_static = false;  // analytic density on the grid, no particles
+  bool frozen = false;     // evolution = false: the push leaves it alone
 };
 
 // ------------------------------------------------------------ helpers
@@ -1085,9 +1087,18 @@ extern "C" int qp_species_download_q3(qp_species* sp, int pos, float* rf) {
 }
 
 // ------------------------------------------------------------------ beam
+// init_fdist3d_0xx conversions of a beam's keys to cells and its charge per
+// particle, then the profile's loader (fdist3d_class.f03:222-1166).
 extern "C" int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out) {
   if (!ctx || !d || !out) return fail(ctx, __LINE__, "null argument");
-  if (d->profile != 0) return fail(ctx, __LINE__, "only the tri-Gaussian beam profile 0 is supported");
+  const int pf = d->profile;
+  if (pf != 0 && pf != 1 && pf != 2 && pf != 3 && pf != 100)
+    return fail(ctx, __LINE__, "beam profile must be 0, 1, 2, 3 or 100");
+  if (d->static_density && pf != 0 && pf != 1)
+    return fail(ctx, __LINE__, "only beam profiles 0 and 1 can be static");
+  if (pf <= 2 && (d->np[0] < 1 || d->np[1] < 1 || d->np[2] < 1))
+    return fail(ctx, __LINE__, "beam np must be at least 1 in each direction");
+  if (!(d->q != 0.f)) return fail(ctx, __LINE__, "beam q must not be 0");
   const GridDims& g = ctx->g;
   float lo[3], hi[3];
   for (int a = 0; a < 3; ++a) {
@@ -1104,8 +1115,6 @@ extern "C" int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out)
   L.nx = g.nx;
   L.ny = g.ny;
   L.nz = ctx->nz;
-  L.qm = beam_charge(d->q, d->peak_density, d->sigma, lo, hi, g.indx, g.indy, ctx->indz, L.npx,
-                     L.npy, L.npz);
   L.vtx = d->sigma_v[0];
   L.vty = d->sigma_v[1];
   L.vtz = d->sigma_v[2];
@@ -1117,23 +1126,107 @@ extern "C" int qp_beam_create(qp_ctx* ctx, const qp_beam_desc* d, qp_beam** out)
   L.y0 = (d->center[1] - lo[1]) / dy;
   L.z0 = (d->center[2] - lo[2]) / dz;
   L.quiet = d->quiet_start != 0;
-  L.npmax = d->npmax > 0 ? d->npmax : (long long)L.npx * L.npy * L.npz + 8;
+  // centroid polynomials in cells: c1 dz dz / dx, c2 dz / dx, c3 / dx
+  L.cx[0] = d->centroid_x[0] * dz * dz / dx;
+  L.cx[1] = d->centroid_x[1] * dz / dx;
+  L.cx[2] = d->centroid_x[2] / dx;
+  L.cy[0] = d->centroid_y[0] * dz * dz / dy;
+  L.cy[1] = d->centroid_y[1] * dz / dy;
+  L.cy[2] = d->centroid_y[2] / dy;
+  const long long nfull = (long long)L.npx * L.npy * L.npz;
+  L.npmax = d->npmax > 0 ? d->npmax : nfull + 8;
   std::vector<float> c[7];
+  long long n = 0;
   int ierr = 0;
-  const long long n = beam_random(ctx->rng, L, c, &ierr);
-  if (ierr) return fail(ctx, __LINE__, "PRVDIST32_RANDOM: npmax too small");
+  bool outside = false;  // a profile-1 beam whose z range misses the box
+  if (pf == 0) {
+    L.qm = beam_charge(d->q, d->peak_density, d->sigma, lo, hi, g.indx, g.indy, ctx->indz, L.npx,
+                       L.npy, L.npz);
+    if (!d->static_density) n = beam_random(ctx->rng, L, c, &ierr);
+  } else if (pf == 1) {
+    if (d->npiece < 2 || !d->piecewise_z || !d->piecewise_fz)
+      return fail(ctx, __LINE__, "beam profile 1 needs at least 2 piecewise points");
+    const std::vector<float> z(d->piecewise_z, d->piecewise_z + d->npiece);
+    const std::vector<float> fz(d->piecewise_fz, d->piecewise_fz + d->npiece);
+    float sumz = 0.f;
+    if (!beam_zprofile(z, fz, lo[2], dz, ctx->nz, &L.zf, &sumz))
+      return fail(ctx, __LINE__, "Piecewise_z is not monotonically increasing");
+    L.qm = beam_charge_q(d->q, d->peak_density, 1.f, d->sigma[0], d->sigma[1], sumz, dx, dy, dz,
+                         L.npx, L.npy, L.npz);
+    outside = (z.front() - lo[2]) / dz >= (float)ctx->nz || (z.back() - lo[2]) / dz <= 0.f;
+    if (!d->static_density && !outside) {
+      Uniform uni(d->seed ? d->seed : 0x5eedull);
+      n = beam_ran_pfl(ctx->rng, uni, L, c, &ierr);
+    }
+  } else if (pf == 2) {
+    const float sx = std::sqrt(d->beta[0] * d->emittance[0] / d->gamma);
+    const float sy = std::sqrt(d->beta[1] * d->emittance[1] / d->gamma);
+    L.qm = beam_charge_q(d->q, d->peak_density, 1.5f, sx, sy, d->sigma[2], dx, dy, dz, L.npx,
+                         L.npy, L.npz);
+    L.alphax = d->alpha[0];
+    L.alphay = d->alpha[1];
+    L.betax = d->beta[0] / dx;
+    L.betay = d->beta[1] / dy;
+    L.emitx = d->emittance[0] / dx;
+    L.emity = d->emittance[1] / dy;
+    if (!(L.betax > 0.f && L.betay > 0.f && L.emitx > 0.f && L.emity > 0.f && d->gamma > 0.f))
+      return fail(ctx, __LINE__, "beam profile 2 needs beta, emittance and gamma > 0");
+    n = beam_twiss(ctx->rng, L, c, &ierr);
+  } else if (pf == 3) {
+    if (!d->file_name || d->np[0] < 0 || !(d->n0 > 0.f))
+      return fail(ctx, __LINE__, "beam profile 3 needs file_name, np[0] >= 0 and n0 > 0");
+    const float cwp = 5.32150254f * 1e9f / std::sqrt(d->n0);
+    std::string err;
+    n = beam_file(d->file_name, d->np[0], L.x0, L.y0, cwp, dx, dy, dz, g.nx, g.ny, ctx->nz, c,
+                  &err);
+    if (n < 0) return fail(ctx, __LINE__, err);
+    if (d->npmax > 0 && n > d->npmax) ierr = (int)(n - d->npmax);
+  } else {
+    if (d->ppc[0] < 1 || d->ppc[1] < 1 || d->ppc[2] < 1 || !(d->r2 != 0.f))
+      return fail(ctx, __LINE__, "beam profile 100 needs ppc >= 1 and r2 != 0");
+    const float qm = d->q / std::fabs(d->q) / (float)d->ppc[0] / (float)d->ppc[1] /
+                     (float)d->ppc[2];
+    const float bc[3] = {L.x0, L.y0, L.z0};
+    const float* rg[3] = {d->range_x, d->range_y, d->range_z};
+    const float del[3] = {dx, dy, dz};
+    float lb[3], ub[3];
+    for (int a = 0; a < 3; ++a) {
+      lb[a] = (rg[a][0] - lo[a]) / del[a];
+      ub[a] = (rg[a][1] - lo[a]) / del[a];
+    }
+    n = beam_ring(d->ppc, qm, d->peak_density, d->gamma, bc, lb, ub, d->r1 / dx, d->r2 / dx, g.nx,
+                  g.ny, ctx->nz, c);
+    if (d->npmax > 0 && n > d->npmax) ierr = (int)(n - d->npmax);
+  }
+  if (ierr) return fail(ctx, __LINE__, "beam loader: npmax too small");
   qp_beam* b = new qp_beam();
   b->ctx = ctx;
   b->b.np = n;
   b->cap = n;
   b->qbm = d->q / d->m;
+  b->is_static = d->static_density != 0;
+  b->frozen = d->frozen != 0 || b->is_static;
   for (int k = 0; k < BCOMP; ++k) {
     b->b.c[k] = dalloc(n, false);
     if (!b->b.c[k]) return fail(ctx, __LINE__, "out of device memory");
-    CK(cudaMemcpy(b->b.c[k], c[k].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    if (n > 0)
+      CK(cudaMemcpy(b->b.c[k], c[k].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
   }
   b->q3d = dalloc((size_t)(ctx->nz + 1) * g.rplane);
   if (!b->q3d) return fail(ctx, __LINE__, "out of device memory");
+  if (b->is_static && !outside) {
+    // dist3d_000/001 with static = true: the density np q/|q| times the
+    // profile on nodes x < nx, y < ny of slices 1..nz
+    const float amp = d->peak_density * L.qm / std::fabs(L.qm);
+    const float sigz = d->sigma[2] / dz;
+    std::vector<float> plane(g.rplane, 0.f);
+    for (int k = 0; k < ctx->nz; ++k) {
+      beam_static_plane(amp, L.x0, L.y0, L.z0, L.sigx, L.sigy, sigz, L.cx, L.cy,
+                        pf == 1 ? L.zf : std::vector<float>(), g.nx, g.ny, k, g.rp, plane.data());
+      CK(cudaMemcpy(b->q3d + (size_t)k * g.rplane, plane.data(), sizeof(float) * g.rplane,
+                    cudaMemcpyHostToDevice));
+    }
+  }
   *out = b;
   return 0;
 }
@@ -1153,6 +1246,7 @@ extern "C" long long qp_beam_np(const qp_beam* b) { return b->b.np; }
 extern "C" int qp_beam_qdp(qp_beam* b) {
   qp_ctx* ctx = b->ctx;
   const GridDims& g = ctx->g;
+  if (b->is_static) return 0;  // qdeposit_beam3d skips static beams
   CK(cudaMemsetAsync(b->q3d, 0, sizeof(float) * (size_t)(ctx->nz + 1) * g.rplane, ctx->stream));
   launch_beam_deposit(b->b, g, ctx->nz, b->q3d, ctx->st, ctx->stream);
   CK(cudaGetLastError());

@@ -95,7 +95,15 @@ class _BeamDesc(C.Structure):
     _fields_ = [("profile", C.c_int), ("np", C.c_int * 3), ("q", C.c_float), ("m", C.c_float),
                 ("gamma", C.c_float), ("peak_density", C.c_float), ("quiet_start", C.c_int),
                 ("center", C.c_float * 3), ("sigma", C.c_float * 3),
-                ("sigma_v", C.c_float * 3), ("npmax", C.c_longlong)]
+                ("sigma_v", C.c_float * 3), ("npmax", C.c_longlong),
+                ("centroid_x", C.c_float * 3), ("centroid_y", C.c_float * 3),
+                ("static_density", C.c_int), ("frozen", C.c_int), ("npiece", C.c_int),
+                ("ppc", C.c_int * 3), ("piecewise_z", C.POINTER(C.c_float)),
+                ("piecewise_fz", C.POINTER(C.c_float)), ("file_name", C.c_char_p),
+                ("seed", C.c_ulonglong), ("alpha", C.c_float * 2), ("beta", C.c_float * 2),
+                ("emittance", C.c_float * 2), ("n0", C.c_float), ("range_x", C.c_float * 2),
+                ("range_y", C.c_float * 2), ("range_z", C.c_float * 2), ("r1", C.c_float),
+                ("r2", C.c_float), ("reserved", C.c_float * 1)]
 
 
 class _SimDesc(C.Structure):
@@ -382,21 +390,58 @@ class Species2d:
 
 
 class Beam3d:
-    """beam3d with a tri-Gaussian (profile 0) distribution."""
+    """beam3d with one of the fdist3d profiles: 0 tri-Gaussian, 1 Gaussian with a
+    piecewise longitudinal profile, 2 Twiss parameters, 3 particles read from a
+    file, 100 ring (fdist3d_class.f03).  Keys follow beam(i) of the input file;
+    `np3` is np(1:3) (for profile 3 the particle count np); `static` puts the
+    analytic density of profiles 0 and 1 on the grid; `evolution=False` keeps
+    the beam where it is at the push."""
 
     def __init__(self, ctx: Context, np3, q=-1.0, m=1.0, gamma=20000.0, peak_density=1.0,
                  quiet_start=True, center=(0, 0, 0), sigma=(1, 1, 1), sigma_v=(0, 0, 0),
-                 npmax=0):
+                 npmax=0, profile=0, centroid_x=(0, 0, 0), centroid_y=(0, 0, 0),
+                 static=False, evolution=True, piecewise_z=None, piecewise_fz=None, seed=0,
+                 alpha=(0, 0), beta=(0, 0), emittance=(0, 0), sigmaz=None, sigma_vz=None,
+                 file_name=None, n0=0.0, range_x=(0, 0), range_y=(0, 0), range_z=(0, 0),
+                 ppc=(1, 1, 1), r1=0.0, r2=0.0):
         d = _BeamDesc()
-        d.profile = 0
+        d.profile = int(profile)
+        if np.ndim(np3) == 0:
+            np3 = (int(np3), 1, 1)
+        sigma, sigma_v = list(sigma), list(sigma_v)
+        if sigmaz is not None:
+            sigma[2] = sigmaz
+        if sigma_vz is not None:
+            sigma_v[2] = sigma_vz
         for a in range(3):
             d.np[a] = int(np3[a])
             d.center[a], d.sigma[a], d.sigma_v[a] = center[a], sigma[a], sigma_v[a]
+            d.centroid_x[a], d.centroid_y[a] = centroid_x[a], centroid_y[a]
+            d.ppc[a] = int(ppc[a])
         d.q, d.m, d.gamma, d.peak_density = q, m, gamma, peak_density
         d.quiet_start = 1 if quiet_start else 0
         d.npmax = int(npmax)
+        d.static_density = 1 if static else 0
+        d.frozen = 0 if evolution else 1
+        keep = []
+        if piecewise_z is not None:
+            z = np.ascontiguousarray(piecewise_z, dtype=np.float32)
+            fz = np.ascontiguousarray(piecewise_fz, dtype=np.float32)
+            assert z.shape == fz.shape
+            keep += [z, fz]
+            d.npiece = z.size
+            d.piecewise_z = z.ctypes.data_as(C.POINTER(C.c_float))
+            d.piecewise_fz = fz.ctypes.data_as(C.POINTER(C.c_float))
+        d.seed = int(seed)
+        for a in range(2):
+            d.alpha[a], d.beta[a], d.emittance[a] = alpha[a], beta[a], emittance[a]
+            d.range_x[a], d.range_y[a], d.range_z[a] = range_x[a], range_y[a], range_z[a]
+        if file_name is not None:
+            d.file_name = str(file_name).encode()
+        d.n0, d.r1, d.r2 = n0, r1, r2
         h = C.c_void_p()
         ctx._check(ctx._L.qp_beam_create(ctx.h, C.byref(d), C.byref(h)))
+        del keep
         self.ctx, self.h = ctx, h
 
     def np(self):
