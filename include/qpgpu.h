@@ -371,6 +371,35 @@ int qp_sim_download_lineout(qp_sim* sim, int comp, float* out);
 int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double* ms, int* count,
                    double* bytes, int max);
 
+/* ------------------------------------------------------ batched scan */
+
+/* A parameter scan over independent instances (a density, current or beam
+ * size scan): n simulations, each on its own context, advanced by `steps` 3D
+ * steps each.  `workers` host threads take instances from a queue, largest
+ * first, and step them on their own streams, so the instances' kernels
+ * overlap on the GPU; workers <= 0 (or > n) runs one per instance, 1 steps
+ * the instances one after another.  The scan is timed on the device, from a
+ * start event every instance stream waits on to the last instance's end. */
+typedef struct {
+  int steps;
+  int workers;
+} qp_scan_desc;
+
+typedef struct {
+  double gpu_ms;              /* device time of the whole scan */
+  long long particle_slices;  /* sum over instances and steps of Np * nz */
+  int workers;                /* worker threads used */
+  int failed;                 /* instances whose step returned an error */
+} qp_scan_stats;
+
+int qp_scan_run(qp_sim* const* sims, int n, const qp_scan_desc* d, qp_scan_stats* out);
+/* Autotuner of the scan's concurrency: times probe_steps steps of every
+ * instance with 1, 2, 4, ... and n workers and returns the count with the
+ * highest particle-slices per second (and that rate).  The probes advance
+ * the instances by probe_steps times the number of candidates. */
+int qp_scan_tune(qp_sim* const* sims, int n, int probe_steps, int* best_workers,
+                 double* best_rate);
+
 #ifdef __cplusplus
 }
 #endif

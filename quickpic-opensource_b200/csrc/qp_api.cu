@@ -1310,3 +1310,4 @@ extern "C" int qp_beam_download_q3d(qp_beam* b, float* rf) {
 }
 
 #include "qp_sim.inc"
+#include "qp_scan.inc"

@@ -548,3 +548,46 @@ class Simulation:
         if getattr(self, "h", None):
             self.ctx._L.qp_sim_destroy(self.h)
             self.h = None
+
+
+class _ScanDesc(C.Structure):
+    _fields_ = [("steps", C.c_int), ("workers", C.c_int)]
+
+
+class ScanStats(C.Structure):
+    _fields_ = [("gpu_ms", C.c_double), ("particle_slices", C.c_longlong),
+                ("workers", C.c_int), ("failed", C.c_int)]
+
+
+def _sim_array(sims):
+    if not sims:
+        raise QPError("scan: no instances")
+    arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
+    return arr
+
+
+def scan_run(sims, steps=1, workers=0) -> ScanStats:
+    """Advance independent simulations (each on its own Context) by `steps` 3D
+    steps; `workers` host threads step them concurrently on their own streams
+    (0 = one per instance, 1 = one after another).  Device-timed."""
+    L = lib()
+    d = _ScanDesc(int(steps), int(workers))
+    st = ScanStats()
+    rc = L.qp_scan_run(_sim_array(sims), len(sims), C.byref(d), C.byref(st))
+    if rc < 0:
+        msg = L.qp_ctx_last_error(None)
+        raise QPError(msg.decode() if msg else f"qpgpu error {rc}")
+    return st
+
+
+def scan_tune(sims, probe_steps=1):
+    """The autotuner of the scan's concurrency: (best worker count, its
+    particle-slices/s).  Advances every instance by probe_steps per candidate."""
+    L = lib()
+    w = C.c_int(0)
+    r = C.c_double(0.0)
+    rc = L.qp_scan_tune(_sim_array(sims), len(sims), int(probe_steps), C.byref(w), C.byref(r))
+    if rc < 0:
+        msg = L.qp_ctx_last_error(None)
+        raise QPError(msg.decode() if msg else f"qpgpu error {rc}")
+    return w.value, r.value
