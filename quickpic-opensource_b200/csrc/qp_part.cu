@@ -194,7 +194,8 @@ __device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, 
                                           float idex, AmjOut* o) {
   float amx = 1.f - dxp;
   const float amy = 1.f - dyp;
-  const float inv_part_7 = 1.f / p7;
+  // __frcp_rn is the correctly rounded 1/x: the same bits as 1.f / x
+  const float inv_part_7 = __frcp_rn(p7);
   const float qtmh1 = qtmh * inv_part_7;
   const float qtmh2 = qtmh1 * p6;
   float dx = gather(sf[0], nn, mm, amx, amy, dxp, dyp);
@@ -208,7 +209,7 @@ __device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, 
   const float acx = vx + ddx, acy = vy + ddy;
   const float omzt = qtmh1 * oz;
   const float omt = omzt * omzt;
-  const float anorm = 2.f / (1.f + omt);
+  const float anorm = 2.f * __frcp_rn(1.f + omt);  // = 2.f / (1.f + omt): 2 x is exact
   const float rot1 = 0.5f * (1.f - omt);
   const float rot2 = omzt;
   float v1 = (rot1 * acx + rot2 * acy) * anorm + ddx;
@@ -243,23 +244,22 @@ __device__ __forceinline__ void amjdp_one(float (*sf)[TN * TN], int nn, int mm, 
   o->v[7] = v3;
 }
 
-// Add a run's 8 x 4 corner sums (times scale) to the global planes: fire-and-
-// forget reductions in L2 (red.global.add.f32), native for FP32, where a
+// Add a run's 8 x 4 corner sums to the global planes: fire-and-forget
+// reductions in L2 (red.global.add.f32), native for FP32, where a
 // shared-memory float atomic is a compare-and-swap loop.  The top edge of the
 // top tile row folds onto row 0 (the single-rank guard add, PPNACGUARD2L).
 __device__ __forceinline__ void deposit_run(float* const* pl, const TileGeom& tg, int noffp,
-                                            int moffp, int cell, const float (*acc)[4],
-                                            float scale) {
+                                            int moffp, int cell, const float (*acc)[4]) {
   const int nn = cell % TN, mm = cell / TN;
   const long long o0 = (long long)(moffp + mm) * tg.rp + noffp + nn;
   const int y1 = moffp + mm + 1;
   const long long o2 = (long long)(y1 == tg.ny ? 0 : y1) * tg.rp + noffp + nn;
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    atomicAdd(pl[q] + o0, acc[q][0] * scale);
-    atomicAdd(pl[q] + o0 + 1, acc[q][1] * scale);
-    atomicAdd(pl[q] + o2, acc[q][2] * scale);
-    atomicAdd(pl[q] + o2 + 1, acc[q][3] * scale);
+    atomicAdd(pl[q] + o0, acc[q][0]);
+    atomicAdd(pl[q] + o0 + 1, acc[q][1]);
+    atomicAdd(pl[q] + o2, acc[q][2]);
+    atomicAdd(pl[q] + o2 + 1, acc[q][3]);
   }
 }
 
@@ -345,23 +345,29 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
         amjdp_one(sf, nn, mm, dxp, dyp, vxs[j], vys[j], p6s[j], p7s[j], qms[j], qbm, qtmh, dti,
                   dex, idex, &o);
         p6o[j] = o.p6;
+        // the moments only feed the deposit: the scale goes on the corner
+        // weights and the run sums use fused multiply-adds (FP32 roundoff of
+        // the sums, like the order of the reductions)
+        float ws[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ws[r] = o.w[r] * scale;
         const int c = mm * TN + nn;
         if (c != cell) {
-          if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc, scale);
+          if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc);
           cell = c;
 #pragma unroll
           for (int q = 0; q < 8; ++q)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) acc[q][r] = o.v[q] * o.w[r];
+            for (int r = 0; r < 4; ++r) acc[q][r] = o.v[q] * ws[r];
         } else {
 #pragma unroll
           for (int q = 0; q < 8; ++q)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) acc[q][r] += o.v[q] * o.w[r];
+            for (int r = 0; r < 4; ++r) acc[q][r] = __fmaf_rn(o.v[q], ws[r], acc[q][r]);
         }
       }
     }
-    if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc, scale);
+    if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc);
     P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
     *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
     if (ext)
@@ -475,7 +481,7 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
         const float acx = pc[2] + dx, acy = pc[3] + dy, acz = pc[4] + dz;
         const float omxt = qtmh1 * ox, omyt = qtmh1 * oy, omzt = qtmh1 * oz;
         float omt = omxt * omxt + omyt * omyt + omzt * omzt;
-        const float anorm = 2.f / (1.f + omt);
+        const float anorm = 2.f * __frcp_rn(1.f + omt);  // = 2.f / (1.f + omt)
         omt = 0.5f * (1.f - omt);
         float rot4 = omxt * omyt, rot7 = omxt * omzt, rot8 = omyt * omzt;
         const float rot1 = omt + omxt * omxt, rot5 = omt + omyt * omyt, rot9 = omt + omzt * omzt;
