@@ -174,10 +174,23 @@ __global__ void __launch_bounds__(256) k_xinv(XJob job, GridDims g, LineTables t
   const XComp c = job.c[blockIdx.y];
   if (c.cursor_stride && !cursor_ok(c, st)) return;
   const int y0 = blockIdx.x * 8;
-  for (int idx = threadIdx.x; idx < (n + 1) * 8; idx += 256) {
-    const int r = idx & 7, kx = idx >> 3;
-    const int yy = y0 + r;
-    smem[r * pitch + kx] = (yy <= g.ny) ? c.src[(long long)kx * g.kp + yy] : 0.f;
+  // the 8 rows' [kx][y] entries, 32 bytes per kx: batches of 8 loads per
+  // thread are all issued before their shared-memory stores, so a thread waits
+  // for L2 twice per 16 loads instead of once per load
+  const int total = (n + 1) * 8;
+  for (int b0 = threadIdx.x; b0 < total; b0 += 8 * 256) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = b0 + u * 256;
+      const int yy = y0 + (idx & 7);
+      v[u] = (idx < total && yy <= g.ny) ? c.src[(long long)(idx >> 3) * g.kp + yy] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = b0 + u * 256;
+      if (idx < total) smem[(idx & 7) * pitch + (idx >> 3)] = v[u];
+    }
   }
   __syncthreads();
   float* L = smem + warp * pitch;

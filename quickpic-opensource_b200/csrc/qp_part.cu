@@ -42,6 +42,31 @@ __device__ __forceinline__ void stage(float* s, const float* plane, const TileGe
   }
 }
 
+// Stage the same 17 x 17 nodes of np planes (np <= NP; all kernels here run
+// 256 threads): every thread issues all its loads from L2 before its first
+// store to shared memory, so the planes cost one wait instead of one per load.
+template <int NP>
+__device__ __forceinline__ void stage_planes(float (*s)[TN * TN], const float* const (&pl)[NP],
+                                             int np, const TileGeom& tg, int noffp, int moffp) {
+  constexpr int PER = (TN * TN + 255) / 256;
+  float v[NP][PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = threadIdx.x + 256 * k;
+    const int a = i % TN, b = i / TN;
+    const long long o = (long long)(moffp + b) * tg.rp + noffp + a;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) v[p][k] = (i < TN * TN && p < np) ? pl[p][o] : 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = threadIdx.x + 256 * k;
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+      if (i < TN * TN && p < np) s[p][i] = v[p][k];
+  }
+}
+
 // Add a run's 4 corner charges to the global plane q with L2 reductions
 // (red.global.add.f32), folding the top edge of the top tile row onto row 0.
 __device__ __forceinline__ void deposit_q(float* q, const TileGeom& tg, int noffp, int moffp,
@@ -283,14 +308,11 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   const int t = blockIdx.x;
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
-  stage(sf[0], f.fx, tg, noffp, moffp);
-  stage(sf[1], f.fy, tg, noffp, moffp);
-  stage(sf[2], f.bx, tg, noffp, moffp);
-  stage(sf[3], f.by, tg, noffp, moffp);
-  stage(sf[4], f.bz, tg, noffp, moffp);
-  stage(sf[5], f.psit, tg, noffp, moffp);
   const bool ext = f.psi != nullptr;
-  if (ext) stage(sf[6], f.psi, tg, noffp, moffp);
+  {
+    const float* const planes[7] = {f.fx, f.fy, f.bx, f.by, f.bz, f.psit, f.psi};
+    stage_planes<7>(sf, planes, ext ? 7 : 6, tg, noffp, moffp);
+  }
   __syncthreads();
   const float qtmh = 0.5f * qbm * dt;
   const float dti = 1.f / dt;
@@ -407,12 +429,8 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
   if (MODE != 2) {
-    stage(sf[0], f.fx, tg, noffp, moffp);
-    stage(sf[1], f.fy, tg, noffp, moffp);
-    stage(sf[2], f.bx, tg, noffp, moffp);
-    stage(sf[3], f.by, tg, noffp, moffp);
-    stage(sf[4], f.bz, tg, noffp, moffp);
-    stage(sf[5], f.psit, tg, noffp, moffp);
+    const float* const planes[6] = {f.fx, f.fy, f.bx, f.by, f.bz, f.psit};
+    stage_planes<6>(sf, planes, 6, tg, noffp, moffp);
     __syncthreads();
     if (f.combine) {
       // the slice's final force: fxy = -fxy + (bxyz(2), -bxyz(1)), simulation_class.f03:722-724
