@@ -467,8 +467,11 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
       cellr[r] = -1;
       if (k >= n) continue;
       float pc[NCOMP];
+      // with re-binning the kernel never writes A: read-only loads, which
+      // the compiler may issue ahead of the previous round's stores
 #pragma unroll
-      for (int c = 0; c < NCOMP; ++c) pc[c] = A.c[c][base + k];
+      for (int c = 0; c < NCOMP; ++c)
+        pc[c] = MODE != 0 ? __ldg(A.c[c] + base + k) : A.c[c][base + k];
       if (MODE != 2) {
         const float x = pc[0], y = pc[1];
         int nn = (int)x, mm = (int)y;

@@ -68,6 +68,18 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   // phase 2: the solves of the slice start, mode by mode
   for (int ky = threadIdx.x; ky <= n; ky += blockDim.x) {
     const long long o = co + ky;
+    // every global read of the mode first, so they wait for L2 together
+    const float cx = a.cu_x[o], cy = a.cu_y[o], cz = a.cu_z[o];
+    float ex = a.epw_x[o], ey = a.epw_y[o];
+    float ex0 = 0.f, ey0 = 0.f, ex00 = 0.f, ey00 = 0.f;
+    if (a.epw_prev_x) {
+      ex0 = a.epw_prev_x[o];
+      ey0 = a.epw_prev_y[o];
+      if (a.epw_prev2_x) {
+        ex00 = a.epw_prev2_x[o];
+        ey00 = a.epw_prev2_y[o];
+      }
+    }
     const float q = line[0][ky], qb = line[1][ky];
     float ebx, eby;
     k_elf(K, kx, ky, qb, &ebx, &eby);
@@ -76,17 +88,14 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
     const float psi = k_pot(K, kx, ky, q);
     float fx, fy;
     k_grad(K, kx, ky, psi, &fx, &fy);
-    const float cx = a.cu_x[o], cy = a.cu_y[o], cz = a.cu_z[o];
     const float psit = QM(k_pot(K, kx, ky, k_div(K, kx, ky, cx, cy)), -a.dex);
     float bx, by, bz;
     k_bf(K, kx, ky, cx, cy, cz, &bx, &by, &bz);
-    float ex = a.epw_x[o], ey = a.epw_y[o];
     if (a.epw_prev_x) {
       const float ex1 = ex, ey1 = ey;
-      const float ex0 = a.epw_prev_x[o], ey0 = a.epw_prev_y[o];
       if (a.epw_prev2_x) {
-        ex = QA(QM(3.f, QS(ex1, ex0)), a.epw_prev2_x[o]);
-        ey = QA(QM(3.f, QS(ey1, ey0)), a.epw_prev2_y[o]);
+        ex = QA(QM(3.f, QS(ex1, ex0)), ex00);
+        ey = QA(QM(3.f, QS(ey1, ey0)), ey00);
         a.epw_prev2_x[o] = ex0;
         a.epw_prev2_y[o] = ey0;
       } else {
@@ -162,7 +171,9 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
     const float cx = line[0][ky], cy = line[1][ky], cz = line[2][ky];
     float dcx = line[3][ky], dcy = line[4][ky];
     const float axx = line[5][ky], ayy = line[6][ky], axy = line[7][ky];
+    // every global read of the mode first, so they wait for L2 together
     const float ex0 = b.epw_x[o], ey0 = b.epw_y[o];
+    const float ebx = b.epwb_x[o], eby = b.epwb_y[o];
     float ex = ex0, ey = ey0;
     k_bfqp(K, kx, ky, b.aa, b.idex, cz, &dcx, &dcy, axx, ayy, axy, &ex, &ey);
     b.epw_x[o] = ex;
@@ -176,7 +187,7 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
     const float psit = QM(k_pot(K, kx, ky, k_div(K, kx, ky, cx, cy)), -b.dex);
     float bx, by, bz;
     k_bf(K, kx, ky, cx, cy, cz, &bx, &by, &bz);
-    k_assemble_mode(ex, ey, b.epwb_x[o], b.epwb_y[o], b.dex, &bx, &by, &bz);
+    k_assemble_mode(ex, ey, ebx, eby, b.dex, &bx, &by, &bz);
     line[0][ky] = psit;
     line[1][ky] = bx;
     line[2][ky] = by;

@@ -31,8 +31,10 @@ struct KCoef {
   float dnx, dny;  // 6.28318530717959 / (2 n), rounded to FP32 as the reference does
   const float* ffre;
   const float* ffim;
-  __device__ __forceinline__ float re(int kx, int ky) const { return ffre[kx * ny + ky]; }
-  __device__ __forceinline__ float im(int kx, int ky) const { return ffim[kx * ny + ky]; }
+  // the form-factor tables are constant for the context's lifetime: read-only
+  // loads, which the compiler may issue ahead of the kernels' stores
+  __device__ __forceinline__ float re(int kx, int ky) const { return __ldg(ffre + kx * ny + ky); }
+  __device__ __forceinline__ float im(int kx, int ky) const { return __ldg(ffim + kx * ny + ky); }
   __device__ __forceinline__ bool interior(int kx, int ky) const {
     return kx > 0 && kx < nx && ky > 0 && ky < ny;
   }
