@@ -193,7 +193,13 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
   float4* by4 = reinterpret_cast<float4*>(by);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
        i += (long long)gridDim.x * blockDim.x) {
+    // every load of the iteration first, so the thread waits for L2 once
     const float4 vfx = fx4[i], vfy = fy4[i], vbx = bx4[i], vby = by4[i];
+    float4 vpt = make_float4(0.f, 0.f, 0.f, 0.f), vbz = vpt;
+    if (store) {
+      vpt = reinterpret_cast<const float4*>(psit)[i];
+      vbz = reinterpret_cast<const float4*>(bz)[i];
+    }
     float4 f1, f2, b1, b2;
     // f1 = (-fx + by) * dex, f2 = (-fy - bx) * dex; b1 = bx * dex, b2 = by * dex
     f1.x = (-1.f * vfx.x + vby.x) * dex;
@@ -213,10 +219,10 @@ __global__ void k_store3d(GridDims g, float* fx, float* fy, float* bx, float* by
     if (store) {
       reinterpret_cast<float4*>(be.p[0])[pl4 + i] = f1;
       reinterpret_cast<float4*>(be.p[1])[pl4 + i] = f2;
-      reinterpret_cast<float4*>(be.p[2])[pl4 + i] = reinterpret_cast<const float4*>(psit)[i];
+      reinterpret_cast<float4*>(be.p[2])[pl4 + i] = vpt;
       reinterpret_cast<float4*>(bb.p[0])[pl4 + i] = b1;
       reinterpret_cast<float4*>(bb.p[1])[pl4 + i] = b2;
-      reinterpret_cast<float4*>(bb.p[2])[pl4 + i] = reinterpret_cast<const float4*>(bz)[i];
+      reinterpret_cast<float4*>(bb.p[2])[pl4 + i] = vbz;
     }
     if (zero_q) reinterpret_cast<float4*>(zero_q)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }

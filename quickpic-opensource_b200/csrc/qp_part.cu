@@ -33,15 +33,6 @@ __device__ __forceinline__ void tile_origin(const TileGeom& tg, int t, int* noff
   *moffp = TILE * ty;
 }
 
-// stage nodes [noffp, noffp+16] x [moffp, moffp+16] of a plane
-__device__ __forceinline__ void stage(float* s, const float* plane, const TileGeom& tg, int noffp,
-                                      int moffp) {
-  for (int i = threadIdx.x; i < TN * TN; i += blockDim.x) {
-    const int a = i % TN, b = i / TN;
-    s[i] = plane[(long long)(moffp + b) * tg.rp + noffp + a];
-  }
-}
-
 // Stage the same 17 x 17 nodes of np planes (np <= NP; all kernels here run
 // 256 threads): every thread issues all its loads from L2 before its first
 // store to shared memory, so the planes cost one wait instead of one per load.
@@ -148,7 +139,10 @@ __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const fl
   const int t = blockIdx.x;
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
-  stage(sp, psi, tg, noffp, moffp);
+  {
+    const float* const planes[1] = {psi};
+    stage_planes<1>(reinterpret_cast<float(*)[TN * TN]>(sp), planes, 1, tg, noffp, moffp);
+  }
   __syncthreads();
   const float dx2 = dex * dex;
   const int n = P.count[t];
@@ -712,8 +706,12 @@ __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg
       continue;
     }
     const long long src = ib0 + si;
+    // all loads before the stores, so the mover waits for L2 once
+    float v[NCOMP];
 #pragma unroll
-    for (int c = 0; c < NCOMP; ++c) B.c[c][ob + i] = ib.c[c][src];
+    for (int c = 0; c < NCOMP; ++c) v[c] = ib.c[c][src];
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) B.c[c][ob + i] = v[c];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
