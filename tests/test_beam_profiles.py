@@ -360,3 +360,45 @@ def test_frozen_and_static_beams_in_a_step(qp):
         b.close()
     sp.close()
     c.close()
+
+
+@pytest.mark.gpu
+def test_beam_profile_edge_cases(qp, tmp_path):
+    """Beams that miss the box load no particles; bad descriptors are errors,
+    not faults."""
+    c = _ctx(qp)
+    # profile 1 whose piecewise z range lies behind the box: npp = 0 (dist3d_001)
+    b1 = qp.Beam3d(c, (8, 8, 8), profile=1, piecewise_z=[20.0, 30.0],
+                   piecewise_fz=[1.0, 1.0], sigma=(0.5, 0.5, 0.0))
+    assert b1.np() == 0
+    b1.qdp()
+    assert not np.any(b1.get_q3d())
+    b1.close()
+    # ring whose y range misses the box: no particles (dist3d_100)
+    b2 = qp.Beam3d(c, (1, 1, 1), profile=100, ppc=(1, 1, 1), range_x=(-3.0, 3.0),
+                   range_y=(20.0, 30.0), range_z=(1.0, 2.0), r1=1.0, r2=0.5)
+    assert b2.np() == 0
+    b2.close()
+    # errors: unknown profile, non-increasing piecewise z, missing file, static profile 2
+    with pytest.raises(qp.QPError, match="profile must be"):
+        qp.Beam3d(c, (8, 8, 8), profile=4)
+    with pytest.raises(qp.QPError, match="monotonically"):
+        qp.Beam3d(c, (8, 8, 8), profile=1, piecewise_z=[2.0, 1.0], piecewise_fz=[1.0, 1.0])
+    with pytest.raises(qp.QPError, match="cannot open"):
+        qp.Beam3d(c, 10, profile=3, file_name=tmp_path / "missing.txt", n0=1e16)
+    with pytest.raises(qp.QPError, match="static"):
+        qp.Beam3d(c, (8, 8, 8), profile=2, static=True, alpha=(0, 0), beta=(1, 1),
+                  emittance=(1, 1))
+    # a short file is an error
+    short = tmp_path / "short.txt"
+    short.write_text("-100 0 0 20000 0 0 -1\n")
+    with pytest.raises(qp.QPError, match="read beam file"):
+        qp.Beam3d(c, 3, profile=3, file_name=short, n0=1e16)
+    # commas and Fortran d exponents read like blanks and e
+    ok = tmp_path / "fortran.txt"
+    ok.write_text("-1.0d2, 0.0, 0.0, 2.0D4, 0.0, 0.0, -1.0\n")
+    b3 = qp.Beam3d(c, 1, profile=3, file_name=ok, n0=1e16)
+    p = b3.get_particles()
+    assert p.shape == (7, 1) and p[5, 0] == np.float32(2.0e4) and p[6, 0] == np.float32(-1.0)
+    b3.close()
+    c.close()
