@@ -282,6 +282,35 @@ __device__ __forceinline__ void deposit_run(float* const* pl, const TileGeom& tg
   }
 }
 
+// deposit_run for a lane's last run, merged across lanes: the right corners
+// of the previous lane's last run are added to this run's left corners when
+// take is set, and this run's right corners are left to the next lane when
+// give is set.  Every lane of the warp must call it (the shuffles); a lane
+// with no run (cell < 0) only passes values on.
+__device__ __forceinline__ void deposit_last(float* const* pl, const TileGeom& tg, int noffp,
+                                             int moffp, int cell, const float (*acc)[4],
+                                             bool take, bool give) {
+  const unsigned full = 0xffffffffu;
+  const int c = cell < 0 ? 0 : cell;
+  const int nn = c % TN, mm = c / TN;
+  const long long o0 = (long long)(moffp + mm) * tg.rp + noffp + nn;
+  const int y1 = moffp + mm + 1;
+  const long long o2 = (long long)(y1 == tg.ny ? 0 : y1) * tg.rp + noffp + nn;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float r1 = __shfl_up_sync(full, acc[q][1], 1);
+    const float r3 = __shfl_up_sync(full, acc[q][3], 1);
+    if (cell >= 0) {
+      atomicAdd(pl[q] + o0, take ? acc[q][0] + r1 : acc[q][0]);
+      atomicAdd(pl[q] + o2, take ? acc[q][2] + r3 : acc[q][2]);
+      if (!give) {
+        atomicAdd(pl[q] + o0 + 1, acc[q][1]);
+        atomicAdd(pl[q] + o2 + 1, acc[q][3]);
+      }
+    }
+  }
+}
+
 // Each thread takes 4 consecutive particles (float4 loads of each component)
 // and keeps the deposits of a run of particles in one cell in registers,
 // adding them to the global planes when the cell changes (deposit_run).  With
@@ -318,18 +347,24 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
     return;
   }
   const long long base = (long long)t * P.cap;
-  for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
-    const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
-    const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + base + k0);
-    const float4 VX = *reinterpret_cast<const float4*>(P.c[2] + base + k0);
-    const float4 VY = *reinterpret_cast<const float4*>(P.c[3] + base + k0);
+  const int lane = threadIdx.x & 31;
+  // the whole warp loops while one of its lanes has particles (the shuffles
+  // of the last runs); a lane past the count reads the tile's first slots and
+  // neither deposits nor writes them
+  for (int k0 = 4 * threadIdx.x; k0 - 4 * lane < n; k0 += 4 * blockDim.x) {
+    const bool live = k0 < n;
+    const long long kb = base + (live ? k0 : 0);
+    const float4 X = *reinterpret_cast<const float4*>(P.c[0] + kb);
+    const float4 Y = *reinterpret_cast<const float4*>(P.c[1] + kb);
+    const float4 VX = *reinterpret_cast<const float4*>(P.c[2] + kb);
+    const float4 VY = *reinterpret_cast<const float4*>(P.c[3] + kb);
     // with ext, p6 and p7 are formed here from psi (k_extpsi) instead of read
     float4 P6 = make_float4(0.f, 0.f, 0.f, 0.f), P7 = P6;
     if (!ext) {
-      P6 = *reinterpret_cast<const float4*>(P.c[5] + base + k0);
-      P7 = *reinterpret_cast<const float4*>(P.c[6] + base + k0);
+      P6 = *reinterpret_cast<const float4*>(P.c[5] + kb);
+      P7 = *reinterpret_cast<const float4*>(P.c[6] + kb);
     }
-    const float4 QM = *reinterpret_cast<const float4*>(P.c[7] + base + k0);
+    const float4 QM = *reinterpret_cast<const float4*>(P.c[7] + kb);
     const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
     const float vxs[4] = {VX.x, VX.y, VX.z, VX.w}, vys[4] = {VY.x, VY.y, VY.z, VY.w};
     float p6s[4] = {P6.x, P6.y, P6.z, P6.w}, p7s[4] = {P7.x, P7.y, P7.z, P7.w};
@@ -383,11 +418,22 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
         }
       }
     }
-    if (cell >= 0) deposit_run(pl, tg, noffp, moffp, cell, acc);
-    P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
-    *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
-    if (ext)
-      *reinterpret_cast<float4*>(P.c[6] + base + k0) = make_float4(p7s[0], p7s[1], p7s[2], p7s[3]);
+    // the last run's right corners go to the next lane when its last run is
+    // in the next cell in x (cell + 1 is never a cell at a tile row's end)
+    const unsigned full = 0xffffffffu;
+    int cprev = __shfl_up_sync(full, cell, 1);
+    int cnext = __shfl_down_sync(full, cell, 1);
+    if (lane == 0) cprev = -1;
+    if (lane == 31) cnext = -1;
+    deposit_last(pl, tg, noffp, moffp, cell, acc, cprev >= 0 && cell == cprev + 1,
+                 cell >= 0 && cnext == cell + 1);
+    if (live) {
+      P6 = make_float4(p6o[0], p6o[1], p6o[2], p6o[3]);
+      *reinterpret_cast<float4*>(P.c[5] + base + k0) = P6;
+      if (ext)
+        *reinterpret_cast<float4*>(P.c[6] + base + k0) =
+            make_float4(p7s[0], p7s[1], p7s[2], p7s[3]);
+    }
   }
 }
 
