@@ -202,8 +202,11 @@ void launch_beam_push(const BeamBuf& b, const GridDims& g, int nz, const Fields3
                       float dtcx, float dtcz, float cofd1, int* keep, DevStatus* st,
                       cudaStream_t s) {
   if (b.np == 0) return;
+  // one particle per thread: the gathers of a particle wait for memory once,
+  // and the many resident CTAs overlap those waits (a grid-stride loop would
+  // wait once per particle of a thread)
   long long blocks = (b.np + 255) / 256;
-  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks > (1LL << 30)) blocks = 1LL << 30;
   k_beam_push<<<(int)blocks, 256, 0, s>>>(b, g, nz, f, qtmh, dtcx, dtcz, cofd1, keep, st);
 }
 
@@ -221,8 +224,8 @@ void launch_beam_scatter(const BeamBuf& src, const int* keep, const int* offsets
 void launch_beam_deposit(const BeamBuf& b, const GridDims& g, int nz, float* q3, DevStatus* st,
                          cudaStream_t s) {
   if (b.np == 0) return;
-  long long blocks = (b.np + 255) / 256;
-  if (blocks > 148 * 32) blocks = 148 * 32;
+  long long blocks = (b.np + 255) / 256;  // one particle per thread, as the push
+  if (blocks > (1LL << 30)) blocks = 1LL << 30;
   k_beam_deposit<<<(int)blocks, 256, 0, s>>>(b, g, nz, q3, st);
 }
 
