@@ -500,18 +500,37 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   int written = 0;  // stayers written to B so far (the same in every thread)
   for (int c0 = 0; c0 < n; c0 += (MODE != 0 ? CH : (int)blockDim.x)) {
     int cellr[NR];
+    // with re-binning the kernel never writes A: its particles are read with
+    // read-only loads, and each round's are requested one round ahead, so
+    // the wait for L2 overlaps the previous round's push
+    float pn[NCOMP];
+    {
+      const int k = c0 + (MODE != 0 ? warp * (CH / 8) + lane : (int)threadIdx.x);
+      if (MODE != 0 && k < n) {
+#pragma unroll
+        for (int c = 0; c < NCOMP; ++c) pn[c] = __ldg(A.c[c] + base + k);
+      }
+    }
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       const int slot = MODE != 0 ? warp * (CH / 8) + r * 32 + lane : threadIdx.x;
       const int k = c0 + slot;
       cellr[r] = -1;
-      if (k >= n) continue;
       float pc[NCOMP];
-      // with re-binning the kernel never writes A: read-only loads, which
-      // the compiler may issue ahead of the previous round's stores
+      if (MODE != 0) {
 #pragma unroll
-      for (int c = 0; c < NCOMP; ++c)
-        pc[c] = MODE != 0 ? __ldg(A.c[c] + base + k) : A.c[c][base + k];
+        for (int c = 0; c < NCOMP; ++c) pc[c] = pn[c];
+        const int kn = k + 32;  // the next round's slot
+        if (r + 1 < NR && kn < n) {
+#pragma unroll
+          for (int c = 0; c < NCOMP; ++c) pn[c] = __ldg(A.c[c] + base + kn);
+        }
+      }
+      if (k >= n) continue;
+      if (MODE == 0) {
+#pragma unroll
+        for (int c = 0; c < NCOMP; ++c) pc[c] = A.c[c][base + k];
+      }
       if (MODE != 2) {
         const float x = pc[0], y = pc[1];
         int nn = (int)x, mm = (int)y;
