@@ -9,8 +9,6 @@ import numpy as np
 import pytest
 from conftest import make_config, rel_l2
 
-pytestmark = pytest.mark.gpu
-
 SIZES = [(6, 6, 4), (5, 5, 4), (6, 6, 5), (5, 5, 5)]
 
 
@@ -42,6 +40,7 @@ def _close(insts):
         c.close()
 
 
+@pytest.mark.gpu
 def test_scan_matches_instances_stepped_alone(qp):
     peaks = [1.0, 2.0, 4.0, 0.5]
     a = [_instance(qp, ind, p) for ind, p in zip(SIZES, peaks)]
@@ -62,6 +61,7 @@ def test_scan_matches_instances_stepped_alone(qp):
     _close(a + b)
 
 
+@pytest.mark.gpu
 def test_scan_tune_and_sequential_workers(qp):
     insts = [_instance(qp, ind, 2.0) for ind in SIZES[:3]]
     sims = [i[3] for i in insts]
@@ -72,6 +72,7 @@ def test_scan_tune_and_sequential_workers(qp):
     _close(insts)
 
 
+@pytest.mark.gpu
 def test_scan_refuses_shared_contexts(qp):
     c, sp, bm, sim = _instance(qp, SIZES[1], 1.0)
     sim2 = qp.Simulation(c, [sp], [bm], iter=2, store3d=True, dt=0.0)
@@ -79,3 +80,26 @@ def test_scan_refuses_shared_contexts(qp):
         qp.scan_run([sim, sim2], steps=1)
     sim2.close()
     _close([(c, sp, bm, sim)])
+
+
+@pytest.mark.parametrize("n", [16, 64])
+def test_scan_instances_follow_the_stated_distribution(n):
+    """bench.py's scan instances (host logic, no GPU): seeded, grids among
+    128^2 / 256^2 / 512^2 with 256 slices, nb/np and sigma_r in their ranges
+    with (nb/np) sigma_r^2 <= 1, beam particles growing with the grid."""
+    import bench
+
+    a, b = bench.scan_instances(n), bench.scan_instances(n)
+    assert a == b
+    seen = set()
+    for cfg in a:
+        ind = cfg["grid"]["ind"]
+        assert ind[0] == ind[1] and ind[0] in (7, 8, 9) and ind[2] == 8
+        seen.add(ind[0])
+        bm = cfg["beams"][0]
+        peak, sr = bm["peak_density"], bm["sigma"][0]
+        assert 0.5 <= peak <= 20.0 and 0.1 <= sr <= 0.5 and peak * sr * sr <= 1.0
+        assert bm["sigma"][2] == 0.5
+        nb = int(np.prod(bm["np"]))
+        assert nb == {7: 262144, 8: 1048576, 9: 2097152}[ind[0]]
+    assert seen == {7, 8, 9}
