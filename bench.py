@@ -71,6 +71,13 @@ CONFIGS = {
                              peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                              sigma=[0.3, 0.3, 0.6],
                              sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the profiling case with the reference's fixed 2 passes
+    "prof_fixed2": dict(grid=dict(ind=[9, 9, 6], box=BOX), iter=2, dt=10.0,
+                        species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                        beams=[dict(np=[256, 256, 16], q=-1.0, m=1.0, gamma=20000.0,
+                                    peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
+                                    sigma=[0.3, 0.3, 0.6],
+                                    sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the small CPU-runnable case (128^3, 2x2 ppc, 262,144 beam particles)
     "small": dict(grid=dict(ind=[7, 7, 7], box=BOX), iter=2, dt=10.0,
                   species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
