@@ -332,6 +332,8 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
   const bool ext = f.psi != nullptr;
+  // the count is read with the field planes, so the two waits overlap
+  const int n = P.count[t];
   {
     const float* const planes[7] = {f.fx, f.fy, f.bx, f.by, f.bz, f.psit, f.psi};
     stage_planes<7>(sf, planes, ext ? 7 : 6, tg, noffp, moffp);
@@ -341,7 +343,6 @@ __global__ void __launch_bounds__(256, 3) k_amjdp(PartBuf P, TileGeom tg, Gather
   const float dti = 1.f / dt;
   const float idex = 1.f / dex;
   const float dx2 = dex * dex;
-  const int n = P.count[t];
   if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
     if (threadIdx.x == 0) raise_error(st, -6);
     return;
@@ -468,6 +469,7 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   const int t = blockIdx.x;
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
+  const int n = A.count[t];  // read with the field planes: the waits overlap
   if (MODE != 2) {
     const float* const planes[6] = {f.fx, f.fy, f.bx, f.by, f.bz, f.psit};
     stage_planes<6>(sf, planes, 6, tg, noffp, moffp);
@@ -489,7 +491,6 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   const float anx = (float)tg.nx, any = (float)tg.ny;
   const float edgelx = (float)noffp, edgerx = (float)(noffp + TILE);
   const float edgely = (float)moffp, edgery = (float)(moffp + TILE);
-  const int n = A.count[t];
   if (n < 0 || n > A.cap) {  // a count beyond the tile's slots: never read past them
     if (threadIdx.x == 0) raise_error(st, -6);
     return;
