@@ -186,8 +186,14 @@ int qp_species_pmove(qp_species* sp);
  * count_out one int per tile; ntiles = (2^indx / 16) * (2^indy / 16).  The
  * output equals qp_species_pmove's on the same input.  The mover inbox and
  * the status live in one fixed device array of
- * QP_PMOVE_STATIC_SCRATCH_BYTES, which every GPU that loads the library holds
- * until the process exits; no call allocates or frees device memory.  The
+ * QP_PMOVE_STATIC_SCRATCH_BYTES, which a GPU holds from the moment the
+ * library first touches the array there until the process exits.  The CUDA
+ * runtime loads the array's module lazily (the default since CUDA 12.2), so
+ * that moment is qp_ctx_create on the device, or else the first
+ * qp_pmove_static call on it: a caller that hands the GPU's memory to its own
+ * allocator makes one of those calls first (or runs with
+ * CUDA_MODULE_LOADING=EAGER, which places the array when the library loads).
+ * After that no call allocates or frees device memory.  The
  * inbox takes min(16384, about 16 MiB / (40 B * ntiles)) movers per tile
  * (408 on a 512 x 512 grid, 100 on 1024 x 1024); grids that leave fewer than
  * QP_PMOVE_STATIC_MIN_INBOX are rejected, and so is a step that moves more

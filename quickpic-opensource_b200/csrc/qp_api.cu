@@ -179,6 +179,9 @@ extern "C" int qp_ctx_create(const qp_grid_desc* grid, int device, qp_ctx** out)
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   if (fft_kernels_init() || part_kernels_init() || slice_kernels_init())
     return fail(ctx, __LINE__, "kernel init failed");
+  // the fixed scratch array of qp_pmove_static is placed on the device with
+  // the context, before a caller's own allocator can take the rest
+  if (pmove_static_reserve()) return fail(ctx, __LINE__, "static scratch set-up failed");
   if (line_tables_build(&ctx->tx, grid->indx)) return fail(ctx, __LINE__, "table alloc failed");
   if (grid->indy == grid->indx)
     ctx->ty = ctx->tx;

@@ -35,7 +35,7 @@ constexpr int kMaxInboxCap = 16384;  // the insert kernel sorts at most this man
 constexpr size_t kBytesPerMover = NCOMP * sizeof(float) + sizeof(unsigned long long);
 
 std::mutex g_setup_mutex;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
+bool g_attr_done[kMaxDevices] = {};
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -44,19 +44,28 @@ int reject(int line, const std::string& msg) {
   return -1;
 }
 
-// Once per device, with that device current: the scratch's device address
-// and the insert kernel's shared-memory limit.
-int setup_device(int dev, unsigned char** out) {
+// The scratch's device address on the current device.  The runtime loads this
+// file's module (and places the array) at the first use of one of its symbols,
+// so the lookup is what reserves the array on a device; it is repeated on
+// every call, which keeps the address right after a context is torn down and
+// re-created (cudaDeviceReset).
+int scratch_address(unsigned char** out) {
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_pmove_scratch);
+  if (e != cudaSuccess)
+    return reject(__LINE__, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = static_cast<unsigned char*>(ptr);
+  return 0;
+}
+
+// Once per device, with that device current: the insert kernel's
+// shared-memory limit (a function attribute; it allocates nothing).
+int setup_device(int dev) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_pmove_scratch);
-    if (e != cudaSuccess)
-      return reject(__LINE__, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  if (!g_attr_done[dev]) {
     if (part_kernels_init() != 0) return reject(__LINE__, "insert kernel attribute set-up failed");
-    g_scratch_ptr[dev] = static_cast<unsigned char*>(ptr);
+    g_attr_done[dev] = true;
   }
-  *out = g_scratch_ptr[dev];
   return 0;
 }
 
@@ -73,6 +82,16 @@ __global__ void k_check_counts(const int* count, int ntiles, int cap, DevStatus*
 }
 
 }  // namespace
+
+namespace qp {
+// Places the static scratch on the current device now, so that a caller who
+// creates a context before handing the rest of the GPU's memory to its own
+// allocator has the array reserved before that allocator takes its pool.
+int pmove_static_reserve() {
+  unsigned char* base = nullptr;
+  return scratch_address(&base);
+}
+}  // namespace qp
 
 extern "C" int qp_pmove_static(int indx, int indy, const float* const* part_in,
                                const int* count_in, int cap_in, float* const* part_out,
@@ -118,7 +137,7 @@ extern "C" int qp_pmove_static(int indx, int indy, const float* const* part_in,
   if (e != cudaSuccess) return reject(__LINE__, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return reject(__LINE__, "pmove_static: device index too large");
   unsigned char* base = nullptr;
-  if (setup_device(dev, &base)) return -1;
+  if (setup_device(dev) || scratch_address(&base)) return -1;
 
   DevStatus* st = reinterpret_cast<DevStatus*>(base);
   Inbox ib{};
@@ -162,8 +181,14 @@ extern "C" int qp_pmove_static(int indx, int indy, const float* const* part_in,
     return reject(__LINE__, "pmove_static: a tile count lies outside 0.." +
                                 std::to_string(cap_in) + " (found " +
                                 std::to_string(h.need_cap) + ")");
+  if (h.error == -4 || h.error == -3)
+    return reject(__LINE__, "pmove_static: a particle position lies outside the grid (code " +
+                                std::to_string(h.error) + ")");
+  if (h.error == -6)
+    return reject(__LINE__, "pmove_static: internal error, a tile's stayer count left its "
+                            "slots (code -6)");
   if (h.error < 0)
-    return reject(__LINE__, "pmove_static: particle position outside the grid (code " +
+    return reject(__LINE__, "pmove_static: internal error in the re-bin kernels (code " +
                                 std::to_string(h.error) + ")");
   if (h.need_inbox > ib.cap)
     return reject(__LINE__, "pmove_static: " + std::to_string(h.need_inbox) +

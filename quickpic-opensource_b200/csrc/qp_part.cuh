@@ -44,6 +44,8 @@ struct GatherPlanes {
 };
 
 int part_kernels_init();
+// places the static scratch of qp_pmove_static on the current device (qp_noalloc.cu)
+int pmove_static_reserve();
 void launch_deposit_rho(const PartBuf& P, const TileGeom& tg, float* q, const DevStatus* st,
                         cudaStream_t s);
 void launch_extpsi(const PartBuf& P, const TileGeom& tg, const float* psi, float qbm, float dex,

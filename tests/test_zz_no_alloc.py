@@ -119,3 +119,66 @@ def test_static_pmove_rejects_and_recovers(env):
     gp, gk = sp.get_particles(max(sp.nppmx, int(counts.max())))
     _check_equal(gp, gk, planes, counts)
     sp.close()
+
+
+def test_static_pmove_rejects_inbox_overflow_and_bad_counts(env):
+    """On a 1024 x 1024 grid (4096 tiles) the fixed array leaves room for 100
+    movers per tile: 200 particles leaving one tile for the same neighbour are
+    refused with the inbox message, and a tile count above cap_in is refused
+    with the tile-count message."""
+    torch, qp, L, ctx = env
+    ix = iy = 10
+    mx1 = (1 << ix) // 16
+    nt = mx1 * mx1
+    cap_in, cap_out = 256, 512
+    pin = [torch.zeros((nt, cap_in), device="cuda") for _ in range(8)]
+    t0 = 10 + mx1 * 10  # tile (10, 10): cells x 160..175, y 160..175
+    rng = np.random.default_rng(5)
+    n = 200
+    pin[0][t0, :n] = torch.from_numpy(rng.uniform(176.5, 191.5, n).astype(np.float32)).cuda()
+    pin[1][t0, :n] = torch.from_numpy(rng.uniform(160.5, 175.5, n).astype(np.float32)).cuda()
+    counts = np.zeros(nt, dtype=np.int32)
+    counts[t0] = n
+    cin = torch.from_numpy(counts).cuda()
+    pout = [torch.full((nt, cap_out), -7.0, device="cuda") for _ in range(8)]
+    cout = torch.zeros(nt, dtype=torch.int32, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    rc = L.qp_pmove_static(ix, iy, _ptrs(pin), C.c_void_p(cin.data_ptr()), cap_in, _ptrs(pout),
+                           C.c_void_p(cout.data_ptr()), cap_out, stream)
+    assert rc < 0
+    msg = L.qp_ctx_last_error(None)
+    assert b"moved into one tile" in msg and b"holds 100" in msg, msg
+    # a count above the input capacity
+    counts[:] = 0
+    counts[7] = cap_in + 1
+    cin2 = torch.from_numpy(counts).cuda()
+    rc = L.qp_pmove_static(ix, iy, _ptrs(pin), C.c_void_p(cin2.data_ptr()), cap_in, _ptrs(pout),
+                           C.c_void_p(cout.data_ptr()), cap_out, stream)
+    assert rc < 0
+    assert b"tile count lies outside" in L.qp_ctx_last_error(None)
+
+
+def test_static_pmove_allocates_nothing(env):
+    """After the array is placed (context creation or a first call), a call
+    leaves the device's free memory unchanged."""
+    torch, qp, L, ctx = env
+    sp = qp.Species2d(ctx, ppc=(2, 2), xtras=0.5)
+    pp, kp = _displaced(sp, 31, 3.0)
+    cap_in, cap_out = pp.shape[1], 2 * pp.shape[1]
+    pin = _planes(torch, pp, cap_in)
+    cin = torch.from_numpy(np.ascontiguousarray(kp, dtype=np.int32)).cuda()
+    pout = [torch.zeros((len(kp), cap_out), device="cuda") for _ in range(8)]
+    cout = torch.zeros(len(kp), dtype=torch.int32, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    args = (6, 6, _ptrs(pin), C.c_void_p(cin.data_ptr()), cap_in, _ptrs(pout),
+            C.c_void_p(cout.data_ptr()), cap_out, stream)
+    assert L.qp_pmove_static(*args) == 0, L.qp_ctx_last_error(None)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert L.qp_pmove_static(*args) == 0, L.qp_ctx_last_error(None)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert int(cout.sum().item()) == int(kp.sum())
+    sp.close()
