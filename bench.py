@@ -17,8 +17,10 @@ wake lineout read back.
 
 --impl reference: the reference's algorithm on the host cores (the CPU oracle,
 QuickPIC's routines restated in C++/OpenMP; the Fortran reference needs gfortran,
-MPI, HDF5 and json-fortran, none of which exist in this image), timed on a
-bounded sample of slices of the same workload.
+MPI, HDF5 and json-fortran, none of which exist in this image), timed over one
+whole 3D step of the same workload.
+The engine's line also carries the error of sampled slices against the FP64
+oracle (fp64_error) and a CPU baseline timed on the same sampled slices.
 Multi-GPU: the path does not shard (slices are a recurrence in xi); --gpus N
 runs N independent replicas, one per GPU, and value is their aggregate.
 """
@@ -249,10 +251,12 @@ def run_engine(args, cfg, rank, world, local_rank, dist):
            "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(line.nbytes),
            "ms_per_step": e_ms / args.steps}
 
-    # ---- roofline of the dominant kernel, from a per-launch profile of 16 slices
-    prof = sim.profile(min(16, nz))
+    # ---- roofline of the dominant kernel: a per-launch profile of one more 3D
+    # step, with every launch of prof_slices slices spread over the box timed
+    prof = sim.profile(min(args.prof_slices, nz))
     peak, peak_kind = load_peaks()
-    top = max(prof.items(), key=lambda kv: kv[1][0])
+    top = max(((k, v) for k, v in prof.items() if not k.endswith(":skipped")),
+              key=lambda kv: kv[1][0])
     name, (ms, cnt, byts) = top
     tot = sum(v[0] for v in prof.values())
     achieved = (byts / cnt) / (ms / cnt * 1e-3) / 1e9 if ms > 0 else 0.0
@@ -265,12 +269,18 @@ def run_engine(args, cfg, rank, world, local_rank, dist):
     kernels = {k: {"ms": round(v[0], 4), "launches": v[1],
                    "GBps": round(v[2] / (v[0] * 1e-3) / 1e9, 1) if v[0] > 0 and v[2] > 0 else None}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    # ---- error against the FP64 oracle, and the CPU baseline, on sampled slices
+    errors = cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        errors, cpu = sampled_slices(cfg, ctx, sp, sim, args.error_samples,
+                                     os.cpu_count() or 1)
     sim.close()
     for b in beams:
         b.close()
     sp.close()
     ctx.close()
     return dict(value=value, t_ms=t_ms, e2e=e2e, roofline=roofline, kernels=kernels,
+                errors=errors, cpu=cpu, prof_slices=args.prof_slices,
                 clocks=clocks.summary(), npl=npl, nz=nz, regrow=regrow,
                 passes_per_slice=passes / (nz * args.steps), unconverged=unconverged,
                 launches=kernels_per_step * args.steps,
@@ -480,28 +490,104 @@ def job_throughput(units_local, t_ms_local, dist):
     return units / (t_ms * 1e-3), t_ms
 
 
-def cpu_slices(cfg, budget_s, max_slices, threads):
-    """Time slices of the oracle (the reference's routines restated, FP32, OpenMP).
+def _oracle_fields(o, nx, ny):
+    """A slice's outputs held by the oracle after it: the stored force
+    (fxy, psit), B (bxy, bz), psi, epw and the extrapolated current."""
+    nxv, nyp = nx + 2, 2 * ny + 1
+    fxy = o.get("fxy").reshape((2, nxv, nyp), order="F")[:, :, : ny + 1]
+    bxyz = o.get("bxyz").reshape((3, nxv, nyp), order="F")[:, :, : ny + 1]
+    return dict(fxy=fxy, psit=o.get("psit").reshape((nxv, nyp), order="F")[:, : ny + 1],
+                bxy=bxyz[0:2], bz=bxyz[2],
+                psi=o.get("psi").reshape((nxv, nyp), order="F")[:, : ny + 1],
+                epw=o.get("epw_k").reshape((2, ny + 1, nx + 1), order="F"),
+                cu_k=o.get("cu_k").reshape((3, ny + 1, nx + 1), order="F"))
 
-    Returns (particle-slices/s, slices timed, seconds, plasma particles)."""
+
+def _engine_fields(sim, j, ny):
+    be, bb = sim.get_plane("bexyz", j), sim.get_plane("bbxyz", j)
+    return dict(fxy=be[0:2], psit=be[2], bxy=bb[0:2], bz=bb[2],
+                psi=sim.get_field("psi")[0, :, : ny + 1], epw=sim.get_field("epw"),
+                cu_k=sim.get_field("cu_k"))
+
+
+def _err(a, b, ref_norm=None):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = ref_norm if ref_norm is not None else np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a))
+
+
+def sampled_slices(cfg, ctx, sp, sim, nsamples, threads):
+    """One more 3D step of the engine, stopped before each of `nsamples`
+    slices spread evenly over the box (slice 1 + floor((2i+1) nz / (2 n))).
+    Before a sampled slice j the engine's state -- tiled particles, the
+    Fourier-space B_perp iterate, the extrapolated current and slice j's beam
+    charge plane -- is handed to the oracle, the engine runs slice j, and the
+    FP32 oracle (the reference's SGL build, timed: the CPU baseline) and the
+    FP64 oracle (its DBL build: the error) run slice j from the same state.
+    Returns (errors, cpu figures)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import oracle
 
-    c = dict(cfg)
-    c["store3d"] = False
-    sim = oracle.Sim(c, np.float32)
+    nx, ny, nz = ctx.nx, ctx.ny, ctx.nz
+    ocfg = dict(cfg, beams=[], store3d=False)
+    o32, o64 = oracle.Sim(ocfg, np.float32), oracle.Sim(ocfg, np.float64)
+    samples = sorted({1 + ((2 * i + 1) * nz) // (2 * nsamples) for i in range(nsamples)})
+    names = ("fxy", "psit", "bxy", "bz", "psi", "epw", "cu_k")
+    e64 = {k: [] for k in names}
+    e32 = {k: [] for k in names}
+    eref = {k: [] for k in names}
+    sq = {k: [0.0, 0.0, 0.0] for k in names}  # sum |engine - fp64|^2, |fp32 - fp64|^2, |fp64|^2
+    t32 = 0.0
+    p0 = int(o32.get("passes")[0])
     sim.begin3d()
-    npl = int(sim.get("np")[0])
-    t0 = time.perf_counter()
-    j = 0
-    while j < max_slices:
-        j += 1
-        sim.slice(j)
-        if time.perf_counter() - t0 >= budget_s and j >= 2:
-            break
-    dt = time.perf_counter() - t0
-    sim.close()
-    return npl * j / dt, j, dt, npl
+    for j in samples:
+        if j > sim.next_slice:
+            sim.slices(j - sim.next_slice)
+        pp, kp = sp.get_particles()
+        st = dict(ppart=pp, kpic=kp, epw_k=sim.get_field("epw"), cu_k=sim.get_field("cu_k"),
+                  qb=sim.get_plane("qb", j))
+        sim.slices(1)
+        got = _engine_fields(sim, j, ny)
+        for o in (o32, o64):
+            o.set_state(**st)
+        t0 = time.perf_counter()
+        o32.slice(j)
+        t32 += time.perf_counter() - t0
+        o64.slice(j)
+        r32, r64 = _oracle_fields(o32, nx, ny), _oracle_fields(o64, nx, ny)
+        bnorm = float(np.linalg.norm(np.asarray(r64["bxy"], dtype=np.float64)))
+        for k in names:
+            ref = bnorm if k == "bz" else None
+            e64[k].append(_err(got[k], r64[k], ref))
+            e32[k].append(_err(got[k], r32[k], ref))
+            eref[k].append(_err(r32[k], r64[k], ref))
+            a64 = np.asarray(r64[k], dtype=np.float64)
+            sq[k][0] += float(np.sum((np.asarray(got[k], np.float64) - a64) ** 2))
+            sq[k][1] += float(np.sum((np.asarray(r32[k], np.float64) - a64) ** 2))
+            sq[k][2] += bnorm ** 2 if k == "bz" else float(np.sum(a64 ** 2))
+    passes32 = int(o32.get("passes")[0]) - p0
+    if sim.next_slice <= nz:
+        sim.slices(nz - sim.next_slice + 1)
+    sim.end3d()
+    o32.close()
+    o64.close()
+    npl = sp.np()
+    errors = {"samples": samples,
+              "vs_fp64_oracle": {k: float(np.sqrt(v[0] / v[2])) for k, v in sq.items()},
+              "fp32_oracle_vs_fp64_oracle": {k: float(np.sqrt(v[1] / v[2]))
+                                             for k, v in sq.items()},
+              "vs_fp64_oracle_max_slice": {k: float(max(v)) for k, v in e64.items()},
+              "fp32_oracle_vs_fp64_max_slice": {k: float(max(v)) for k, v in eref.items()},
+              "vs_fp32_oracle_max_slice": {k: float(max(v)) for k, v in e32.items()},
+              "note": "relative L2 from identical inputs (the engine's state before each "
+                      "sampled slice): vs_fp64_oracle pools all samples, *_max_slice is the "
+                      "worst single slice; bz against |B_perp| (roundoff-level in an "
+                      "axisymmetric wake); the FP32 oracle (the reference's SGL arithmetic) "
+                      "is shown against the FP64 oracle for scale"}
+    cpu = {"value": npl * len(samples) / t32, "seconds": t32, "slices": len(samples),
+           "passes_per_slice": passes32 / len(samples) if cfg.get("tol", 0.0) > 0 else cfg["iter"]}
+    return errors, cpu
 
 
 def workload_desc(cfg, name):
@@ -523,30 +609,49 @@ def passes_desc(cfg):
 
 
 def run_reference(args, cfg):
+    """The reference's algorithm on the host cores: the CPU oracle (QuickPIC's
+    routines restated in C++, FP32 like the reference's SGL build, OpenMP on
+    every host core) runs one whole 3D step of the same workload -- the beam
+    deposit, every slice with the same B passes and tolerance, the beam push,
+    the species renew -- timed end to end.  The particles are loaded before the
+    timer, as the engine's are.  One medium step takes minutes on the host, so
+    the step is not repeated K times: the line reports the one step it timed
+    (timed_3d_steps), after W slices of the small case as warm-up."""
     threads = os.cpu_count() or 1
-    npl = plasma_count(cfg)
-    per_step = max(2, args.ref_slices)
-    # each step: a bounded sample of `per_step` slices of the same 3D step
-    for _ in range(args.warmup):
-        cpu_slices(cfg, 0.0, 2, threads)
-    vals, secs, nsl = [], 0.0, 0
-    for _ in range(args.steps):
-        v, j, dt, npl = cpu_slices(cfg, 1e9, per_step, threads)
-        vals.append(v)
-        secs += dt
-        nsl += j
-    value = npl * nsl / secs
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    warm = oracle.Sim(dict(CONFIGS["small"], store3d=False), np.float32)
+    warm.begin3d()
+    for j in range(1, max(1, args.warmup) + 1):
+        warm.slice(j)
+    warm.close()
+    c = dict(cfg)
+    c["store3d"] = True  # the beam push reads the stored 3D fields
+    sim = oracle.Sim(c, np.float32)
+    npl = int(sim.get("np")[0])
+    nz = 1 << cfg["grid"]["ind"][2]
+    t0 = time.perf_counter()
+    sim.step3d()
+    secs = time.perf_counter() - t0
+    passes = int(sim.get("passes")[0]) if cfg.get("tol", 0.0) > 0 else nz * cfg["iter"]
+    unconv = int(sim.get("unconverged")[0])
+    sim.close()
+    value = npl * nz / secs
+    sample = (f"one whole {args.config} 3D step (beam deposit, {nz} slices, beam push, renew) "
+              f"in {secs:.1f} s; CPU restatement of the reference algorithm (FP32, OpenMP, "
+              f"{threads} threads), not the Fortran binary")
     line = {"impl": "reference", "metric": "plasma particle-slices/s", "value": value,
             "unit": "particle-slices/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+            "warmup": args.warmup, "timed_3d_steps": 1, "ms_per_step": secs * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded reference loaders)",
-            "config": {"workload": workload_desc(cfg, args.config), "parallelism": "replicas"},
+            "config": {"workload": workload_desc(cfg, args.config), "plasma_particles": npl,
+                       "slices": nz, "iter": cfg["iter"], "tol": cfg.get("tol", 0.0),
+                       "passes_per_slice": round(passes / nz, 3),
+                       "unconverged_slices": unconv, "parallelism": "replicas"},
             "cpu_baseline": {"value": value, "unit": "particle-slices/s", "cores": threads,
-                             "kind": "port",
-                             "sample": f"{per_step} slices per step of the {args.config} 3D step "
-                                       f"(CPU restatement of the reference algorithm, FP32, "
-                                       f"OpenMP; not the Fortran binary)"},
+                             "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "particle-slices/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -559,8 +664,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--config", default="medium", choices=sorted(CONFIGS))
-    ap.add_argument("--ref-slices", type=int, default=4)
-    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--prof-slices", type=int, default=32,
+                    help="slices of the profiled step whose launches are timed")
+    ap.add_argument("--error-samples", type=int, default=24,
+                    help="slices of one step checked against the FP64 oracle (and timed on "
+                    "the FP32 oracle for the CPU baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default="step", choices=["step", "fft", "amjdp", "push", "scan"],
                     help="step: the 3D step (the benchmark); fft: transform kernels alone; "
@@ -597,12 +705,15 @@ def main():
         dist = tdist
     r = run_engine(args, cfg, rank, world, local_rank, dist)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        v, j, dt, npl = cpu_slices(cfg, args.cpu_budget, 64, threads)
-        cpu = {"value": v, "unit": "particle-slices/s", "cores": threads, "kind": "port",
-               "sample": f"first {j} slices of one {args.config} 3D step in {dt:.1f} s "
-                         f"(CPU restatement of the reference algorithm, FP32, OpenMP)"}
+    if rank == 0 and r["cpu"] is not None:
+        c = r["cpu"]
+        cpu = {"value": c["value"], "unit": "particle-slices/s", "cores": os.cpu_count() or 1,
+               "kind": "port", "passes_per_slice": round(c["passes_per_slice"], 3),
+               "sample": f"{c['slices']} slices spread evenly over one {args.config} 3D step "
+                         f"(head, beam and wake), each run by the oracle from the engine's "
+                         f"state before it, {c['seconds']:.1f} s of slice time (CPU restatement "
+                         f"of the reference algorithm, FP32, OpenMP; the beam deposit and "
+                         f"push are not in this sample, --impl reference times a whole step)"}
     if rank == 0:
         line = {"metric": "plasma particle-slices/s", "value": r["value"],
                 "unit": "particle-slices/s", "n_gpus": world, "steps": args.steps,
@@ -618,6 +729,7 @@ def main():
                            "parallelism": "replicas" if world > 1 else "single"},
                 "step_time_ms": r["t_ms"] / args.steps,
                 "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": cpu,
+                "fp64_error": r["errors"],
                 "gpu_launches": r["launches"], "clocks": r["clocks"],
                 "regrowths": r["regrow"], "kernels": r["kernels"]}
         print(json.dumps(line), flush=True)

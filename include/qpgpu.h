@@ -5,7 +5,7 @@
  * push and deposits (species2d / part2d), the 2D sine/cosine Poisson and B
  * solves (field2d / fpois2d / fft2d) and the beam 3D deposit (beam3d / part3d)
  * on one GPU.  A Fortran caller binds these entry points with iso_c_binding
- * (the binding module is shown in INTEGRATION.md); every argument is a plain
+ * (bind(C) interfaces, one per function); every argument is a plain
  * pointer, integer or float, and no call retains a host pointer after it
  * returns.  Each function below names the reference routine it replaces
  * (paths relative to QuickPIC-OpenSource/source).
@@ -317,7 +317,8 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * vpot = 1 (with store3d = 1, one species) also keeps the vector potential
  * vpot3d of every slice (simulation_class.f03:711-716: field2d%vpot of the
  * last pass's current, fftkr, times -dex), downloaded as "vpot";
- * use_graphs is accepted and ignored: the slices are launched directly;
+ * use_graphs is kept for binary compatibility and ignored: the slices are
+ * launched directly;
  * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
  * step with beam3d%push of every beam with the stored bexyz, bbxyz
  * (simulation_class.f03:753-757), dt = 0 leaves the beams where they are. */
@@ -351,11 +352,41 @@ int qp_sim_destroy(qp_sim* sim);
  * remaining ones keep their order.  With one pipeline stage part3d%pmove
  * (PMOVE32) has nothing to move, so this is the whole beam3d%push. */
 int qp_beam_push(qp_beam* b, qp_sim* sim, float dt);
-/* One 3D step; `stats` may be NULL.  The species are renewed at the end. */
+/* One 3D step; `stats` may be NULL.  The species are renewed at the end.
+ * Equal to qp_sim_begin3d, qp_sim_slices(nz), qp_sim_end3d. */
 int qp_sim_step3d(qp_sim* sim, qp_step_stats* stats);
+/* The 3D step in the three parts of go_simulation, so that a caller can stop
+ * between slices (to read or restore the state a slice hands to the next):
+ * qp_sim_begin3d = the start of the step (simulation_class.f03:611-641: beam
+ * deposits, the fields handed to slice 1, the slice cursor at 1);
+ * qp_sim_slices = the next n slices of the loop 643-736 (grow-and-retry
+ * included; between calls the species' live particles are in the buffer
+ * that qp_species_download/upload read and write);
+ * qp_sim_end3d = the end of the step (741-764: beam push when dt > 0,
+ * species renew), once all nz slices have run; `stats` as qp_sim_step3d
+ * (gpu_ms spans begin3d to end3d, caller pauses included).
+ * qp_sim_next_slice = the slice the next qp_sim_slices call starts with
+ * (1-based), 0 when no step is in progress. */
+int qp_sim_begin3d(qp_sim* sim);
+int qp_sim_slices(qp_sim* sim, int n);
+int qp_sim_end3d(qp_sim* sim, qp_step_stats* stats);
+int qp_sim_next_slice(const qp_sim* sim);
+/* The Fourier-space fields a slice hands to the next, reference k-space
+ * layout (dim, ny+1, nx+1): "epw" (transverse-B iterate, dim 2), "cu_k"
+ * (current after the xi extrapolation, dim 3), and with predict > 0
+ * "epw_prev" / "epw_prev2" (B_perp of earlier slices, dim 2).  With the
+ * species particles they are the whole state between two slices; download
+ * them with qp_sim_download_field. */
+int qp_sim_upload_field(qp_sim* sim, const char* name, const float* in);
+/* One plane (0-based index 0..nz) of a 3D array, reference layout: "bexyz",
+ * "bbxyz", "vpot" (3, nx+2, ny+1) and "q3" (nx+2, ny+1) as stored by the
+ * slice of that index (store3d = 1); "qb" (nx+2, ny+1) the beam charge
+ * plane the slice of that index reads (ufield3d%copyadd in qdpcopy,
+ * simulation_class.f03:645-650). */
+int qp_sim_download_plane(qp_sim* sim, const char* name, int plane, float* out);
 /* Fields of the last slice (real space or Fourier space, reference layout):
  * name = "psi", "fxy", "bxyz", "psit", "cu", "dcu", "amu" (rs) or
- * "epw", "cu_k", "epwb" (ks). */
+ * "epw", "cu_k", "epwb", "epw_prev", "epw_prev2" (ks). */
 int qp_sim_download_field(qp_sim* sim, const char* name, float* out);
 /* 3D fields (3, nx+2, ny+1, nz+1): "bexyz" or "bbxyz"; species 3D charge
  * (nx+2, ny+1, nz+1): "q3". */
@@ -365,15 +396,18 @@ int qp_sim_download_3d(qp_sim* sim, const char* name, float* out);
  * field that the reference's field slice diagnostics write to HDF5 files
  * (init_diag, simulation_class.f03:771-1100), read here without a file. */
 int qp_sim_download_lineout(qp_sim* sim, int comp, float* out);
-/* Per-kernel device times of the first `nslices` slices of a 3D step, run
- * without graphs with an event pair around every launch (the timing side of
- * the reference's per-step ELOG stamps, simulation_class.f03:614-645).
- * Kernel names are written newline-separated into `names`; ms[i], count[i] and
- * bytes[i] are the total milliseconds, launches and algorithmic bytes
- * (minimal FP32 traffic of the work done) of name i.  Under a convergence
- * tolerance the profiled slices run two fixed passes, so that every timed
- * launch does its work.  Returns the number of names (<= max), or < 0 on
- * error.  The species are renewed afterwards. */
+/* Per-kernel device times of one whole 3D step (the timing side of the
+ * reference's per-step ELOG stamps, simulation_class.f03:614-645), with
+ * `nslices` slices sampled at an even stride across the box (slice
+ * 1 + floor((2i+1) nz / (2 nslices)), i = 0..nslices-1) and an event pair
+ * around every launch of a sampled slice.  The step runs under the
+ * simulation's own settings, tolerance included, and advances it by one 3D
+ * step.  Kernel names are written newline-separated into `names`; ms[i],
+ * count[i] and bytes[i] are the total milliseconds, launches and
+ * algorithmic bytes (minimal FP32 traffic of the work done) of name i.
+ * Under a tolerance, launches of passes after the one at which their slice
+ * stopped return at once and are reported as "<kernel>:skipped" with no
+ * bytes.  Returns the number of names (<= max), or < 0 on error. */
 int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double* ms, int* count,
                    double* bytes, int max);
 

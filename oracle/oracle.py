@@ -390,7 +390,8 @@ P_FIXED = 22
 B_NPAR = 18
 W = dict(psi=1, fxy=2, bxyz=3, psit=4, cu=5, dcu=6, amu=7, epw_k=8, cu_k=9, qe=10, qb=11,
          epwb_k=12, ppart=13, kpic=14, bexyz=15, bbxyz=16, q3=17, q3d=18, qn=19, beam0=20,
-         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26, unconverged=27, vpot3d=28)
+         nppmx=21, dcu_k=22, bxyz_k=23, np=24, qsp=25, passes=26, unconverged=27, vpot3d=28, epw_b2=29,
+         epw_b3=30)
 
 
 def sim_params(cfg) -> np.ndarray:
@@ -467,6 +468,33 @@ class Sim:
         rc = self._f("get")(C.c_void_p(self.h), C.c_int(w), _p(out), C.c_longlong(n))
         assert rc == 0, rc
         return out[:n]
+
+    def set(self, what, arr):
+        """Set part of the state one slice hands to the next: "ppart"
+        (8, nppmx, ntiles), "kpic", "epw_k", "cu_k", "epw_b2"/"epw_b3" (the
+        predictor's earlier B_perp) or "qb" (the next slice's beam charge
+        plane, used once)."""
+        a = np.asfortranarray(arr, dtype=self.dtype).ravel(order="F")
+        rc = self._f("set")(C.c_void_p(self.h), C.c_int(W[what]), _p(a), C.c_longlong(a.size))
+        assert rc == 0, (what, rc)
+
+    def set_state(self, ppart, kpic, epw_k, cu_k, qb=None):
+        """The whole state a slice reads from the slice before it: tiled
+        particles ppart(8, nppmx, ntiles) and kpic, the Fourier-space B_perp
+        iterate and extrapolated current, and the beam charge plane of the
+        next slice (nx+2, ny+1) or (nx+2, 2ny+1)."""
+        self.set("ppart", ppart)
+        self.set("kpic", np.asarray(kpic, dtype=np.float64))
+        self.set("epw_k", epw_k)
+        self.set("cu_k", cu_k)
+        if qb is not None:
+            full = np.zeros((qb.shape[0], 2 * self.ny + 1), dtype=np.float64, order="F")
+            full[:, : qb.shape[1]] = qb
+            self.set("qb", full)
+
+    @property
+    def ny(self):
+        return 1 << int(self.cfg["grid"]["ind"][1])
 
     def close(self):
         if self.h:

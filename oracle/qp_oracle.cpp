@@ -2342,6 +2342,9 @@ void pgpost32l(const T* part, int npp, T* q, int nxv, int nypmx) {
   }                                                                                     \
   extern "C" long long oq_sim_size_##S(void* h, int what) {                             \
     return static_cast<OSim<T>*>(h)->size(what);                                        \
+  }                                                                                     \
+  extern "C" int oq_sim_set_##S(void* h, int what, const T* in, long long n) {          \
+    return static_cast<OSim<T>*>(h)->set(what, in, n);                                  \
   }
 
 OQ_DEF(float, f)

@@ -507,11 +507,48 @@ class Simulation:
         self.ctx._check(self.ctx._L.qp_sim_step3d(self.h, C.byref(st)))
         return st
 
+    # the 3D step in the parts of go_simulation (simulation_class.f03:611-764)
+    def begin3d(self):
+        """Beam deposits, the fields handed to slice 1, slice cursor at 1."""
+        self.ctx._check(self.ctx._L.qp_sim_begin3d(self.h))
+
+    def slices(self, n=1):
+        """Run the next n slices of the step."""
+        self.ctx._check(self.ctx._L.qp_sim_slices(self.h, int(n)))
+
+    def end3d(self) -> StepStats:
+        """Beam push (dt > 0) and species renew, after all nz slices."""
+        st = StepStats()
+        self.ctx._check(self.ctx._L.qp_sim_end3d(self.h, C.byref(st)))
+        return st
+
+    @property
+    def next_slice(self):
+        """The slice the next slices() call starts with; 0 outside a step."""
+        return int(self.ctx._L.qp_sim_next_slice(self.h))
+
+    def set_field(self, name, arr):
+        """Restore a field handed from slice to slice ("epw", "cu_k",
+        "epw_prev", "epw_prev2"), reference k-space layout (dim, ny+1, nx+1)."""
+        a = np.asfortranarray(arr, dtype=np.float32)
+        self.ctx._check(self.ctx._L.qp_sim_upload_field(self.h, name.encode(), _ptr(a)))
+
+    def get_plane(self, name, plane):
+        """Plane `plane` (0..nz) of "bexyz", "bbxyz", "vpot" (3, nx+2, ny+1) or
+        "q3", "qb" (nx+2, ny+1)."""
+        c = self.ctx
+        shape = (c.nx + 2, c.ny + 1) if name in ("q3", "qb") else (3, c.nx + 2, c.ny + 1)
+        out = np.zeros(shape, dtype=np.float32, order="F")
+        c._check(c._L.qp_sim_download_plane(self.h, name.encode(), int(plane), _ptr(out)))
+        return out
+
     def get_field(self, name):
         c = self.ctx
-        dims = dict(psi=1, fxy=2, bxyz=3, psit=1, cu=3, dcu=2, amu=3, epw=2, cu_k=3, epwb=2)
+        dims = dict(psi=1, fxy=2, bxyz=3, psit=1, cu=3, dcu=2, amu=3, epw=2, cu_k=3, epwb=2,
+                    epw_prev=2, epw_prev2=2)
         dim = dims[name]
-        shape = c.ks_shape(dim) if name in ("epw", "cu_k", "epwb") else c.rs_shape(dim)
+        ks = ("epw", "cu_k", "epwb", "epw_prev", "epw_prev2")
+        shape = c.ks_shape(dim) if name in ks else c.rs_shape(dim)
         out = np.zeros(shape, dtype=np.float32, order="F")
         c._check(c._L.qp_sim_download_field(self.h, name.encode(), _ptr(out)))
         return out
@@ -534,7 +571,9 @@ class Simulation:
         return out
 
     def profile(self, nslices):
-        """{kernel name: (total ms, launches, algorithmic bytes)} over nslices slices."""
+        """{kernel name: (total ms, launches, algorithmic bytes)} of nslices slices
+        sampled across one whole 3D step (which it runs, advancing the
+        simulation); launches of skipped passes are named "<kernel>:skipped"."""
         buf = C.create_string_buffer(4096)
         ms = (C.c_double * 64)()
         cnt = (C.c_int * 64)()

@@ -28,9 +28,12 @@ def qp():
     return qpgpu
 
 
-@pytest.fixture(scope="module")
-def ctx(qp):
-    c = qp.Context(6, 6, 5, [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]])
+@pytest.fixture(scope="module", params=[(6, 6, 5), (9, 9, 4)], ids=["64sq", "512sq"])
+def ctx(qp, request):
+    """The kernel-level tests run on a 64 x 64 grid (4 x 4 tiles) and on the
+    benchmark's 512 x 512 grid (32 x 32 tiles, 512-point line transforms)."""
+    ix, iy, iz = request.param
+    c = qp.Context(ix, iy, iz, [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]])
     yield c
     c.close()
 
@@ -75,17 +78,27 @@ def test_fftrk_fftkr(qp, ctx, oracle_mod, kind, dim):
     f.close()
 
 
-def test_fft_rectangular_grid(qp, oracle_mod):
+@pytest.mark.parametrize("ix,iy", [(7, 5), (10, 6), (6, 10), (11, 5), (5, 11)])
+def test_fft_rectangular_grid(qp, oracle_mod, ix, iy):
+    """Rectangular grids, and every line length of the transforms: 1024-point
+    lines (the 1024^2 blow-out case) along x and along y, and 2048-point lines,
+    the longest the engine supports; forward and inverse, FP64 oracle."""
     O = oracle_mod
-    c = qp.Context(7, 5, 4, [[-6.0, 6.0], [-3.0, 3.0], [0.0, 10.0]])
-    for kind, dim in ((1, 3), (2, 3)):
-        rs = _rand_rs(O, dim, 7, 5, 7 + kind)
+    c = qp.Context(ix, iy, 4, [[-6.0, 6.0], [-3.0, 3.0], [0.0, 10.0]])
+    ny = 1 << iy
+    for kind, dim in ((1, 3), (2, 3), (3, 3)):
+        rs = _rand_rs(O, dim, ix, iy, 7 + kind)
         f = qp.Field2d(c, dim, 0)
         f.set_rs(rs)
         f.fftrk(kind)
-        k64 = O.ks_zeros(dim, 7, 5, np.float64)
-        O.fftrk(rs.astype(np.float64), k64, kind, 7, 5)
-        assert rel_l2(f.get_ks(), k64) < TOL_FFT64
+        k64 = O.ks_zeros(dim, ix, iy, np.float64)
+        O.fftrk(rs.astype(np.float64), k64, kind, ix, iy)
+        assert rel_l2(f.get_ks(), k64) < TOL_FFT64, kind
+        f.set_ks(k64.astype(np.float32))
+        f.fftkr(kind)
+        r64 = O.rs_zeros(dim, ix, iy, np.float64)
+        O.fftkr(r64, k64.copy(order="F"), kind, ix, iy)
+        assert rel_l2(f.get_rs()[:, :, : ny + 1], r64[:, :, : ny + 1]) < TOL_FFT64, kind
         f.close()
     c.close()
 
@@ -274,11 +287,20 @@ def test_amjdp(qp, ctx, oracle_mod):
     assert np.array_equal(_flat(gp, gk), _flat(pp, kp))
 
 
+def _move_scale(ctx):
+    """Momenta and fields are scaled with the cell size, so that a push moves a
+    particle by the same number of cells (less than a tile, the reference's
+    re-binning limit: PPPORDERF2LA only sends particles to the 8 neighbours)
+    on every grid."""
+    return min(1.0, (0.3125 / 0.1875) * (ctx.dex / ctx.dxi))
+
+
 def test_partpush_then_pmove(qp, ctx, oracle_mod):
     O = oracle_mod
     ix, iy = ctx.indx, ctx.indy
-    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 14, pscale=0.5), ix, iy, xtras=0.5)
-    fxy, bxy, psit = _fields(O, ctx, 50, amp=3.0)
+    m = _move_scale(ctx)
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 14, pscale=0.5 * m), ix, iy, xtras=0.5)
+    fxy, bxy, psit = _fields(O, ctx, 50, amp=3.0 * m)
     sp = _species_with(qp, ctx, pp, kp)
     F, B, P = _upload_fields(qp, ctx, fxy, bxy, psit)
     dex = ctx.dex
@@ -304,8 +326,9 @@ def test_partpush_then_pmove(qp, ctx, oracle_mod):
 def test_fused_push_equals_partpush_pmove(qp, ctx, oracle_mod):
     O = oracle_mod
     ix, iy = ctx.indx, ctx.indy
-    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 15, pscale=0.5), ix, iy, xtras=0.5)
-    fxy, bxy, psit = _fields(O, ctx, 60, amp=3.0)
+    m = _move_scale(ctx)
+    pp, kp, _ = O.bin_particles(_particles(O, ix, iy, 15, pscale=0.5 * m), ix, iy, xtras=0.5)
+    fxy, bxy, psit = _fields(O, ctx, 60, amp=3.0 * m)
     F, B, P = _upload_fields(qp, ctx, fxy, bxy, psit)
     s1 = _species_with(qp, ctx, pp, kp)
     s1.push(F, B, P, ctx.dex)

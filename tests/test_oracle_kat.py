@@ -299,3 +299,36 @@ def test_beam_push_free_streaming_and_drop(oracle_mod):
         assert np.isclose(out[1, k], part[1, src] + py * dt / dex / g, rtol=1e-14)
         dzc = (1.0 + px * px + py * py) / (pz * (pz + g)) * dt / dxi
         assert np.isclose(out[2, k], part[2, src] + dzc, rtol=1e-14)
+
+
+@pytest.mark.parametrize("tol", [0.0, 1e-4], ids=["fixed", "tolerance"])
+def test_slice_from_a_given_state_repeats_the_slice(oracle_mod, tol):
+    """The state one slice hands to the next -- the tiled particles, the
+    Fourier-space B_perp iterate (epw) and the extrapolated current (cu_k) --
+    plus the next slice's beam charge plane is all a slice reads: a fresh
+    oracle given that state repeats slice k+1 of a running one bit for bit.
+    This is what the engine's per-slice parity tests rely on."""
+    O = oracle_mod
+    cfg = make_config(ind=(5, 5, 4), iter=6 if tol else 2)
+    cfg["tol"] = tol
+    a = O.Sim(cfg, np.float64)
+    a.begin3d()
+    k = 7
+    for j in range(1, k + 1):
+        a.slice(j)
+    nx, ny, nz = 32, 32, 16
+    q3d = a.get("q3d").reshape((nx + 2, ny + 1, nz + 1), order="F")
+    nppmx = int(a.get("nppmx")[0])
+    state = dict(ppart=a.get("ppart").reshape((8, nppmx, -1), order="F"), kpic=a.get("kpic"),
+                 epw_k=a.get("epw_k"), cu_k=a.get("cu_k"))
+    c2 = dict(cfg, beams=[], store3d=False)
+    b = O.Sim(c2, np.float64)
+    for name, v in state.items():
+        b.set(name, v)
+    qb = np.zeros((nx + 2, 2 * ny + 1))
+    qb[:, : ny + 1] = q3d[:, :, k + 1]
+    b.set("qb", qb)
+    a.slice(k + 1)
+    b.slice(k + 1)
+    for name in ("psi", "fxy", "bxyz", "psit", "epw_k", "cu_k", "ppart"):
+        assert np.array_equal(a.get(name), b.get(name)), name
