@@ -311,7 +311,8 @@ int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
  * store3d = 1 keeps the 3D fields bexyz, bbxyz and the species q3;
  * predict = 1 starts each slice's B passes from the linear extrapolation
  * 2 epw(j-1) - epw(j-2) of the transverse B of the two previous slices,
- * predict = 2 from the quadratic 3 epw(j-1) - 3 epw(j-2) + epw(j-3), instead
+ * predict = 2 from the quadratic 3 epw(j-1) - 3 epw(j-2) + epw(j-3),
+ * predict = 3 from the learned network (qp_sim_set_predictor), instead
  * of epw(j-1) (the reference's start); with tol > 0 the passes still run to
  * the same tolerance;
  * vpot = 1 (with store3d = 1, one species) also keeps the vector potential
@@ -410,6 +411,67 @@ int qp_sim_download_lineout(qp_sim* sim, int comp, float* out);
  * bytes.  Returns the number of names (<= max), or < 0 on error. */
 int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double* ms, int* count,
                    double* bytes, int max);
+
+/* -------------------------------------------- learned start of the B passes */
+
+/* A convolutional network (5 layers of 3x3 convolutions, 32 channels, BF16
+ * weights and activations, FP32 accumulation, on the BF16 tensor cores) that
+ * predicts the start of each slice's B predictor-corrector passes: a
+ * correction, per Fourier mode, of the linear extrapolation
+ * 2 epw(j-1) - epw(j-2), from epw(j-1), epw(j-2), the current handed to the
+ * slice (cu_k) and the mode coordinates.  It has no counterpart in the
+ * reference, whose passes start from epw(j-1) (simulation_class.f03:676); it
+ * replaces that start when qp_sim_desc.predict = 3, and the passes still run
+ * to the tolerance.  Layer l: weights W[9][cin][cout] (tap = 3 dy + dx, dy and
+ * dx the row and column offsets + 1) then bias[cout]; cin = 16 for layer 1
+ * (9 input features, the rest zero), 32 otherwise; cout = 32, and 16 for
+ * layer 5 (2 outputs used).  An untrained network (seeded He initialisation,
+ * last layer zero) is the linear extrapolation. */
+typedef struct qp_nn qp_nn;
+typedef struct qp_nn_data qp_nn_data;
+int qp_nn_create(int device, unsigned long long seed, qp_nn** out);
+int qp_nn_destroy(qp_nn* nn);
+int qp_nn_num_params(const qp_nn* nn);
+int qp_nn_get_params(qp_nn* nn, float* out);
+int qp_nn_set_params(qp_nn* nn, const float* in);
+/* Forward of nb images in[nb][16][h][w] (w a multiple of 128) to
+ * out[nb][2][h][w] (zero padding at the image edges). */
+int qp_nn_forward(qp_nn* nn, const float* in, int nb, int h, int w, float* out);
+/* Mean squared error of the 2 outputs against target[nb][2][h][w] and its
+ * gradient with respect to every parameter (the parameter layout above). */
+int qp_nn_loss_grad(qp_nn* nn, const float* in, const float* target, int nb, int h, int w,
+                    double* loss, float* grad);
+/* Training pairs recorded from simulations (qp_sim_record): for each slice,
+ * the 128 x 128 low-mode crop of the network's 16 input channels, the target
+ * (the converged epw minus the linear extrapolation, over the epw scale) and
+ * the scale (the RMS of epw(j-1); 0 marks a pair with no field to scale). */
+int qp_nn_data_create(int device, int capacity, qp_nn_data** out);
+int qp_nn_data_destroy(qp_nn_data* t);
+int qp_nn_data_count(const qp_nn_data* t);
+int qp_nn_data_get(qp_nn_data* t, int i, float* img /* [16][128][128] */,
+                   float* target /* [2][128][128] */, float* scale);
+typedef struct {
+  int steps;               /* Adam steps */
+  int batch;               /* pairs per minibatch */
+  float lr;                /* learning rate (x0.3 after half the steps, x0.1 after 3/4) */
+  int reserved;
+  unsigned long long seed; /* minibatch draws */
+} qp_nn_train_desc;
+typedef struct {
+  double first_loss, last_loss; /* minibatch loss at the first and the last step */
+  double gpu_ms;                /* device time of the training */
+  int steps;
+  int reserved;
+} qp_nn_train_stats;
+/* Trains the network on the GPU with its own forward, data-gradient and
+ * weight-gradient kernels. */
+int qp_nn_train(qp_nn* nn, qp_nn_data* t, const qp_nn_train_desc* d, qp_nn_train_stats* st);
+/* Every following slice of `sim` records one training pair into t until it
+ * is full (NULL stops).  Needs nx, ny >= 128 and ny a multiple of 128. */
+int qp_sim_record(qp_sim* sim, qp_nn_data* t);
+/* The network that starts the passes of a simulation created with
+ * predict = 3 (ny a multiple of 128).  The simulation keeps a pointer. */
+int qp_sim_set_predictor(qp_sim* sim, qp_nn* nn);
 
 /* ------------------------------------------------------ batched scan */
 

@@ -21,6 +21,7 @@
 #include "qp_fft.cuh"
 #include "qp_loader.h"
 #include "qp_misc.cuh"
+#include "qp_nn.cuh"
 #include "qp_part.cuh"
 #include "qp_slice.cuh"
 

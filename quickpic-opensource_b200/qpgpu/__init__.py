@@ -31,7 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqpgpu.so")
 
 __all__ = ["QPError", "Context", "Field2d", "Species2d", "Beam3d", "Simulation", "lib",
-           "build", "exported_symbols", "LIB_PATH"]
+           "build", "exported_symbols", "LIB_PATH", "Predictor", "TrainingSet"]
 
 
 class QPError(RuntimeError):
@@ -570,6 +570,17 @@ class Simulation:
         self.ctx._check(self.ctx._L.qp_sim_download_lineout(self.h, comp, _ptr(out)))
         return out
 
+    def record(self, data):
+        """Record one training pair per slice into `data` (a TrainingSet) from
+        the next step on; None stops."""
+        self.ctx._check(self.ctx._L.qp_sim_record(self.h, data.h if data is not None else None))
+        self._rec = data
+
+    def set_predictor(self, net):
+        """The network that starts each slice's passes (predict=3)."""
+        self.ctx._check(self.ctx._L.qp_sim_set_predictor(self.h, net.h))
+        self._net = net
+
     def profile(self, nslices):
         """{kernel name: (total ms, launches, algorithmic bytes)} of nslices slices
         sampled across one whole 3D step (which it runs, advancing the
@@ -630,3 +641,101 @@ def scan_tune(sims, probe_steps=1):
         msg = L.qp_ctx_last_error(None)
         raise QPError(msg.decode() if msg else f"qpgpu error {rc}")
     return w.value, r.value
+
+
+class _TrainDesc(C.Structure):
+    _fields_ = [("steps", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
+                ("reserved", C.c_int), ("seed", C.c_ulonglong)]
+
+
+class TrainStats(C.Structure):
+    _fields_ = [("first_loss", C.c_double), ("last_loss", C.c_double), ("gpu_ms", C.c_double),
+                ("steps", C.c_int), ("reserved", C.c_int)]
+
+
+def _nn_check(rc):
+    if rc < 0:
+        msg = lib().qp_ctx_last_error(None)
+        raise QPError(msg.decode() if msg else f"qpgpu error {rc}")
+    return rc
+
+
+class Predictor:
+    """The learned start of the B passes: 5 layers of 3x3 convolutions (32
+    channels, BF16 tensor cores) on Fourier-space images.  No counterpart in
+    the reference, whose passes start from the previous slice's B
+    (simulation_class.f03:676)."""
+
+    def __init__(self, device=0, seed=1):
+        h = C.c_void_p()
+        _nn_check(lib().qp_nn_create(device, C.c_ulonglong(seed), C.byref(h)))
+        self.h = h
+
+    @property
+    def nparams(self):
+        return int(lib().qp_nn_num_params(self.h))
+
+    def get_params(self):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        _nn_check(lib().qp_nn_get_params(self.h, _ptr(out)))
+        return out
+
+    def set_params(self, p):
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        assert a.size == self.nparams
+        _nn_check(lib().qp_nn_set_params(self.h, _ptr(a)))
+
+    def forward(self, x):
+        """x[nb][16][h][w] (w a multiple of 128) -> out[nb][2][h][w]."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        nb, _, hh, ww = x.shape
+        out = np.zeros((nb, 2, hh, ww), dtype=np.float32)
+        _nn_check(lib().qp_nn_forward(self.h, _ptr(x), nb, hh, ww, _ptr(out)))
+        return out
+
+    def loss_grad(self, x, target):
+        """(mean squared error, gradient of every parameter)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        nb, _, hh, ww = x.shape
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_double(0.0)
+        _nn_check(lib().qp_nn_loss_grad(self.h, _ptr(x), _ptr(t), nb, hh, ww, C.byref(loss),
+                                        _ptr(g)))
+        return loss.value, g
+
+    def train(self, data, steps=500, batch=16, lr=1e-3, seed=7) -> TrainStats:
+        d = _TrainDesc(int(steps), int(batch), float(lr), 0, int(seed))
+        st = TrainStats()
+        _nn_check(lib().qp_nn_train(self.h, data.h, C.byref(d), C.byref(st)))
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().qp_nn_destroy(self.h)
+            self.h = None
+
+
+class TrainingSet:
+    """Training pairs recorded from simulations (Simulation.record)."""
+
+    def __init__(self, capacity, device=0):
+        h = C.c_void_p()
+        _nn_check(lib().qp_nn_data_create(device, int(capacity), C.byref(h)))
+        self.h = h
+
+    def __len__(self):
+        return int(lib().qp_nn_data_count(self.h))
+
+    def get(self, i):
+        """(features [16][128][128], target [2][128][128], scale) of pair i."""
+        img = np.zeros((16, 128, 128), dtype=np.float32)
+        tgt = np.zeros((2, 128, 128), dtype=np.float32)
+        sc = np.zeros(1, dtype=np.float32)
+        _nn_check(lib().qp_nn_data_get(self.h, int(i), _ptr(img), _ptr(tgt), _ptr(sc)))
+        return img, tgt, float(sc[0])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().qp_nn_data_destroy(self.h)
+            self.h = None

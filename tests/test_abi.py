@@ -49,7 +49,8 @@ def test_oracle_is_not_linked_by_the_product(qp):
 STRUCTS = [("qp_grid_desc", "_GridDesc"), ("qp_species_desc", "_SpeciesDesc"),
            ("qp_beam_desc", "_BeamDesc"), ("qp_sim_desc", "_SimDesc"),
            ("qp_step_stats", "StepStats"), ("qp_scan_desc", "_ScanDesc"),
-           ("qp_scan_stats", "ScanStats")]
+           ("qp_scan_stats", "ScanStats"), ("qp_nn_train_desc", "_TrainDesc"),
+           ("qp_nn_train_stats", "TrainStats")]
 
 
 def test_descriptor_layouts_match_the_header(qp, tmp_path):

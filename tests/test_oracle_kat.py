@@ -332,3 +332,41 @@ def test_slice_from_a_given_state_repeats_the_slice(oracle_mod, tol):
     b.slice(k + 1)
     for name in ("psi", "fxy", "bxyz", "psit", "epw_k", "cu_k", "ppart"):
         assert np.array_equal(a.get(name), b.get(name)), name
+
+
+def test_network_oracle_gradient_matches_finite_differences():
+    """The CPU restatement of the predictor network: its backward pass (in
+    float64, no bf16 rounding) agrees with central finite differences of its
+    loss, for parameters of every layer (weights and biases)."""
+    import nn_oracle as N
+
+    rng = np.random.default_rng(3)
+    p = rng.normal(0, 0.3, N.num_params())
+    x = rng.normal(0, 1, (2, 16, 5, 6))
+    t = rng.normal(0, 1, (2, 2, 5, 6))
+    loss, g = N.loss_grad(p, x, t, bf16_rounding=False)
+    offs = np.cumsum([0] + N.layer_sizes())
+    idx = []
+    for l in range(5):
+        idx += list(rng.integers(offs[l], offs[l + 1], 4)) + [offs[l + 1] - 1]
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = N.loss_grad(q, x, t, bf16_rounding=False)
+        q[i] -= 2 * h
+        lm, _ = N.loss_grad(q, x, t, bf16_rounding=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    import nn_oracle as N
+
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, -2.5e-3], dtype=np.float32)
+    r = N.bf16(v)
+    assert r[0] == 1.0
+    assert r[1] == 1.0  # halfway between 1 and 1 + 2^-7: ties to even (1.0)
+    assert r[2] == 1.0 + 2 ** -6  # halfway: ties to the even neighbour 1 + 2^-6
+    assert r[3] == 1.0
+    assert abs(r[4] - -2.5e-3) < 2.5e-3 * 2 ** -8
