@@ -417,16 +417,17 @@ int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double*
 /* A convolutional network (5 layers of 3x3 convolutions, 32 channels, BF16
  * weights and activations, FP32 accumulation, on the BF16 tensor cores) that
  * predicts the start of each slice's B predictor-corrector passes: a
- * correction, per Fourier mode, of the linear extrapolation
- * 2 epw(j-1) - epw(j-2), from epw(j-1), epw(j-2), the current handed to the
- * slice (cu_k) and the mode coordinates.  It has no counterpart in the
+ * correction, per Fourier mode, of the quadratic extrapolation
+ * 3 epw(j-1) - 3 epw(j-2) + epw(j-3), from epw(j-1) and the differences of
+ * the three previous slices' B_perp, the current handed to the slice (cu_k)
+ * and the mode coordinates.  It has no counterpart in the
  * reference, whose passes start from epw(j-1) (simulation_class.f03:676); it
  * replaces that start when qp_sim_desc.predict = 3, and the passes still run
  * to the tolerance.  Layer l: weights W[9][cin][cout] (tap = 3 dy + dx, dy and
  * dx the row and column offsets + 1) then bias[cout]; cin = 16 for layer 1
  * (9 input features, the rest zero), 32 otherwise; cout = 32, and 16 for
  * layer 5 (2 outputs used).  An untrained network (seeded He initialisation,
- * last layer zero) is the linear extrapolation. */
+ * last layer zero) is the quadratic extrapolation. */
 typedef struct qp_nn qp_nn;
 typedef struct qp_nn_data qp_nn_data;
 int qp_nn_create(int device, unsigned long long seed, qp_nn** out);
@@ -443,8 +444,9 @@ int qp_nn_loss_grad(qp_nn* nn, const float* in, const float* target, int nb, int
                     double* loss, float* grad);
 /* Training pairs recorded from simulations (qp_sim_record): for each slice,
  * the 128 x 128 low-mode crop of the network's 16 input channels, the target
- * (the converged epw minus the linear extrapolation, over the epw scale) and
- * the scale (the RMS of epw(j-1); 0 marks a pair with no field to scale). */
+ * (the converged epw minus the quadratic extrapolation, over the epw scale)
+ * and the scale (the RMS of epw(j-1); 0 marks a pair left out of training:
+ * no field to scale, or a target larger than the field itself). */
 int qp_nn_data_create(int device, int capacity, qp_nn_data** out);
 int qp_nn_data_destroy(qp_nn_data* t);
 int qp_nn_data_count(const qp_nn_data* t);

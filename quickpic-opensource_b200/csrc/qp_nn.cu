@@ -198,6 +198,12 @@ __device__ __forceinline__ void unpack8(uint4 u, float* f) {
   }
 }
 
+// The start the network corrects: the quadratic extrapolation of the three
+// previous slices' B_perp, per mode (the engine's predict = 2 start).
+__device__ __forceinline__ float nn_base(float e1, float e0, float em) {
+  return 3.f * (e1 - e0) + em;
+}
+
 // ---------------------------------------------------------------- the kernels
 enum { EPI_RELU = 0, EPI_MASK = 1, EPI_F32 = 2, EPI_EPW = 3 };
 
@@ -372,10 +378,13 @@ __global__ void __launch_bounds__(128) k_conv3x3(const __grid_constant__ CUtenso
       const float sB = a.scale[0];
       const float e1x = a.pl.epw_x[o], e1y = a.pl.epw_y[o];
       const float e0x = a.pl.prev_x[o], e0y = a.pl.prev_y[o];
+      const float emx = a.pl.prev2_x[o], emy = a.pl.prev2_y[o];
+      a.pl.prev2_x[o] = e0x;
+      a.pl.prev2_y[o] = e0y;
       a.pl.prev_x[o] = e1x;
       a.pl.prev_y[o] = e1y;
-      float px = 2.f * e1x - e0x, py = 2.f * e1y - e0y;
-      if (kx >= 1 && ky >= 1) {  // the zero modes kx = 0, ky = 0 take the extrapolation
+      float px = nn_base(e1x, e0x, emx), py = nn_base(e1y, e0y, emy);
+      if (kx >= 1 && ky >= 1) {  // the modes kx = 0, ky = 0 take the extrapolation alone
         px += sB * (acc[0] + a.bias[0]);
         py += sB * (acc[1] + a.bias[1]);
       }
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(128) k_conv3x3(const __grid_constant__ CUtenso
     flag_error(a.err, 1);
   }
   // EPI_EPW: the modes outside the conv image (kx = nx, or ky = ny) take the
-  // linear extrapolation
+  // quadratic extrapolation
   if (EPI == EPI_EPW && blockIdx.x == 0 && !*s_err) {
     for (int i = tid; i < a.ny + 1 + a.nx; i += 128) {
       const int kx = i <= a.ny ? a.nx : i - a.ny - 1;
@@ -401,10 +410,13 @@ __global__ void __launch_bounds__(128) k_conv3x3(const __grid_constant__ CUtenso
       const size_t o = (size_t)kx * a.kp + ky;
       const float e1x = a.pl.epw_x[o], e1y = a.pl.epw_y[o];
       const float e0x = a.pl.prev_x[o], e0y = a.pl.prev_y[o];
+      const float emx = a.pl.prev2_x[o], emy = a.pl.prev2_y[o];
+      a.pl.prev2_x[o] = e0x;
+      a.pl.prev2_y[o] = e0y;
       a.pl.prev_x[o] = e1x;
       a.pl.prev_y[o] = e1y;
-      a.pl.epw_x[o] = 2.f * e1x - e0x;
-      a.pl.epw_y[o] = 2.f * e1y - e0y;
+      a.pl.epw_x[o] = nn_base(e1x, e0x, emx);
+      a.pl.epw_y[o] = nn_base(e1y, e0y, emy);
     }
   }
   __syncthreads();
@@ -644,25 +656,33 @@ __device__ void nn_scales(const float* part, int nx, int ny, float* sc) {
 
 __device__ __forceinline__ float safe_div(float v, float s) { return s > 0.f ? v / s : 0.f; }
 
-// the 16 input channels of mode (kx, ky)
+// the 16 input channels of mode (kx, ky): e1, e1 - e0, e0 - em1 (em1 = e(-1)),
+// cu, coordinates, zeros
 __device__ __forceinline__ void nn_feature(const NNSlicePlanes& p, size_t o, int kx, int ky,
                                            int nx, int ny, const float* sc, float e1x, float e1y,
-                                           float e0x, float e0y, uint4* g0, uint4* g1) {
-  float f[8];
+                                           float e0x, float e0y, float emx, float emy, uint4* g0,
+                                           uint4* g1) {
+  float f[16];
   f[0] = safe_div(e1x, sc[0]);
   f[1] = safe_div(e1y, sc[0]);
-  f[2] = safe_div(e0x, sc[0]);
-  f[3] = safe_div(e0y, sc[0]);
-  f[4] = safe_div(p.cu_x[o], sc[1]);
-  f[5] = safe_div(p.cu_y[o], sc[1]);
-  f[6] = safe_div(p.cu_z[o], sc[2]);
-  f[7] = (float)kx / (float)nx;
+  f[2] = safe_div(e1x - e0x, sc[0]);
+  f[3] = safe_div(e1y - e0y, sc[0]);
+  f[4] = safe_div(e0x - emx, sc[0]);
+  f[5] = safe_div(e0y - emy, sc[0]);
+  f[6] = safe_div(p.cu_x[o], sc[1]);
+  f[7] = safe_div(p.cu_y[o], sc[1]);
+  f[8] = safe_div(p.cu_z[o], sc[2]);
+  f[9] = (float)kx / (float)nx;
+  f[10] = (float)ky / (float)ny;
+  for (int i = NN_FEATURES; i < 16; ++i) f[i] = 0.f;
   g0->x = pack_bf16(f[0], f[1]);
   g0->y = pack_bf16(f[2], f[3]);
   g0->z = pack_bf16(f[4], f[5]);
   g0->w = pack_bf16(f[6], f[7]);
-  g1->x = pack_bf16((float)ky / (float)ny, 0.f);
-  g1->y = g1->z = g1->w = 0u;
+  g1->x = pack_bf16(f[8], f[9]);
+  g1->y = pack_bf16(f[10], f[11]);
+  g1->z = pack_bf16(f[12], f[13]);
+  g1->w = pack_bf16(f[14], f[15]);
 }
 
 // inference: the input image [2][1][nx][ny][8] of the slice; scale_out = epw scale
@@ -677,8 +697,8 @@ __global__ void k_nn_features(NNSlicePlanes p, int nx, int ny, int kp, const flo
     const int kx = (int)(i / ny), ky = (int)(i - (long long)kx * ny);
     const size_t o = (size_t)kx * kp + ky;
     uint4 g0, g1;
-    nn_feature(p, o, kx, ky, nx, ny, sc, p.epw_x[o], p.epw_y[o], p.prev_x[o], p.prev_y[o], &g0,
-               &g1);
+    nn_feature(p, o, kx, ky, nx, ny, sc, p.epw_x[o], p.epw_y[o], p.prev_x[o], p.prev_y[o],
+               p.prev2_x[o], p.prev2_y[o], &g0, &g1);
     reinterpret_cast<uint4*>(img)[i] = g0;
     reinterpret_cast<uint4*>(img)[n + i] = g1;
   }
@@ -692,7 +712,8 @@ struct NNData {
 };
 
 // recording, slice start: the crop's features into slot `slot`, the target
-// slot = -(2 e1 - e0) / scale, the scale; then epw_prev <- epw for every mode
+// slot = -(quadratic start) / scale, the scale; then the history moves one slice on
+// for every mode (epw_prev2 <- epw_prev, epw_prev <- epw)
 __global__ void k_nn_record_start(NNSlicePlanes p, int nx, int ny, int kp, const float* part,
                                   NNData d, int slot) {
   __shared__ float sc[3];
@@ -705,17 +726,20 @@ __global__ void k_nn_record_start(NNSlicePlanes p, int nx, int ny, int kp, const
     const int kx = (int)(i / (ny + 1)), ky = (int)(i - (long long)kx * (ny + 1));
     const size_t o = (size_t)kx * kp + ky;
     const float e1x = p.epw_x[o], e1y = p.epw_y[o], e0x = p.prev_x[o], e0y = p.prev_y[o];
+    const float emx = p.prev2_x[o], emy = p.prev2_y[o];
     if (kx < NN_CROP && ky < NN_CROP) {
       uint4 g0, g1;
-      nn_feature(p, o, kx, ky, nx, ny, sc, e1x, e1y, e0x, e0y, &g0, &g1);
+      nn_feature(p, o, kx, ky, nx, ny, sc, e1x, e1y, e0x, e0y, emx, emy, &g0, &g1);
       const size_t px = (size_t)kx * NN_CROP + ky;
       uint4* im = reinterpret_cast<uint4*>(d.img);
       im[(size_t)slot * C2 + px] = g0;
       im[((size_t)d.cap + slot) * C2 + px] = g1;
       float* t = d.target + (size_t)slot * 2 * C2;
-      t[px] = -safe_div(2.f * e1x - e0x, sc[0]);
-      t[C2 + px] = -safe_div(2.f * e1y - e0y, sc[0]);
+      t[px] = -safe_div(nn_base(e1x, e0x, emx), sc[0]);
+      t[C2 + px] = -safe_div(nn_base(e1y, e0y, emy), sc[0]);
     }
+    p.prev2_x[o] = e0x;
+    p.prev2_y[o] = e0y;
     p.prev_x[o] = e1x;
     p.prev_y[o] = e1y;
   }
@@ -731,6 +755,27 @@ __global__ void k_nn_record_end(NNSlicePlanes p, int kp, NNData d, int slot) {
     const size_t o = (size_t)kx * kp + ky;
     t[i] += safe_div(p.epw_x[o], sB);
     t[C2 + i] += safe_div(p.epw_y[o], sB);
+  }
+}
+
+// recording, after the slice: a pair whose target is larger than the field
+// itself (RMS over the crop above the epw scale: slices where B appears or
+// changes shape abruptly, mostly at the head of the beam) is not a
+// correction the network can learn from; its scale is set to 0, which takes
+// it out of the loss
+__global__ void k_nn_record_validate(NNData d, int slot) {
+  __shared__ float red[32];
+  const size_t C2 = (size_t)NN_CROP * NN_CROP;
+  const float* t = d.target + (size_t)slot * 2 * C2;
+  float v = 0.f;
+  for (size_t i = threadIdx.x; i < 2 * C2; i += blockDim.x) v += t[i] * t[i];
+  for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float s = 0.f;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+    if (!(s / (float)(2 * C2) <= 1.f)) d.scale[slot] = 0.f;
   }
 }
 
@@ -1159,7 +1204,7 @@ extern "C" int qp_nn_create(int device, unsigned long long seed, qp_nn** out) {
     return nn_fail(__LINE__, "out of device memory (network)");
   }
   // He initialisation for the ReLU layers; the last layer starts at zero, so an
-  // untrained network is the linear extrapolation
+  // untrained network is the quadratic extrapolation
   std::vector<float> h(o, 0.f);
   std::mt19937_64 rng(seed);
   for (int l = 0; l < NN_LAYERS - 1; ++l) {
@@ -1518,8 +1563,9 @@ int nn_record_end(NNRuntime* r, void* data, const NNSlicePlanes& p, const GridDi
   if (t->count >= t->d.cap) return 0;
   const int slot = t->count;
   k_nn_record_end<<<64, 256, 0, s>>>(p, g.kp, t->d, slot);
+  k_nn_record_validate<<<1, 1024, 0, s>>>(t->d, slot);
   t->count++;
-  return 1;
+  return 2;
 }
 
 }  // namespace qp

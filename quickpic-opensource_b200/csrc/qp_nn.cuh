@@ -2,9 +2,9 @@
 // convolutional network on Fourier-space images, with BF16 tcgen05 kernels.
 //
 // The predictor maps, for slice j, the Fourier-space B_perp iterates of the
-// two previous slices (epw(j-1), epw(j-2)), the current handed to slice j
+// three previous slices (epw(j-1), epw(j-2), epw(j-3)), the current handed to slice j
 // (cu_k after the xi extrapolation) and the mode coordinates to a correction
-// of the linear extrapolation 2 epw(j-1) - epw(j-2): the start of slice j's
+// of the quadratic extrapolation 3 epw(j-1) - 3 epw(j-2) + epw(j-3): the start of slice j's
 // predictor-corrector passes (the hook at simulation_class.f03:676, where the
 // reference starts from epw(j-1)).  The passes still run to the tolerance.
 //
@@ -26,7 +26,11 @@ constexpr int NN_CIN0 = 16;     // input channels of layer 1 (NN_FEATURES used, 
 constexpr int NN_CH = 32;       // hidden channels
 constexpr int NN_NLAST = 16;    // output channels of layer 5 as computed (NN_OUT used)
 constexpr int NN_OUT = 2;       // the correction of epw_x, epw_y
-constexpr int NN_FEATURES = 9;  // e1.x e1.y e0.x e0.y cu.x cu.y cu.z kx/nx ky/ny
+// e1, e1 - e0, e0 - e(-1) (x and y each, over the epw scale), cu.x, cu.y, cu.z
+// (over their scales), kx/nx, ky/ny: the history enters as differences, so
+// that the network sees slopes and curvatures without the cancellation of
+// nearly equal bfloat16 values
+constexpr int NN_FEATURES = 11;
 constexpr int NN_CROP = 128;    // side of the training crop (the low-mode corner)
 constexpr int NN_NORM_BLOCKS = 148;
 
@@ -42,6 +46,8 @@ struct NNSlicePlanes {
   float* epw_y;
   float* prev_x;         // in: epw(j-2); out: epw(j-1)
   float* prev_y;
+  float* prev2_x;        // in: epw(j-3); out: epw(j-2)
+  float* prev2_y;
   const float* cu_x;     // the current handed to slice j
   const float* cu_y;
   const float* cu_z;
@@ -57,7 +63,7 @@ void nn_runtime_destroy(NNRuntime* r);
 int nn_predict(NNRuntime* r, const void* net, const NNSlicePlanes& p, const GridDims& g,
                DevStatus* st, cudaStream_t s);
 // Recording of training pairs: at the start of slice j (features of the crop,
-// minus the linear extrapolation into the target slot; epw_prev <- epw(j-1)),
+// minus the quadratic extrapolation into the target slot; the history moves on),
 // and at its end (plus the converged epw).  Both skip once the set is full.
 int nn_record_start(NNRuntime* r, void* data, const NNSlicePlanes& p, const GridDims& g,
                     DevStatus* st, cudaStream_t s);
