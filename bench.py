@@ -59,6 +59,15 @@ CONFIGS = {
                                        peak_density=4.0, quiet_start=True,
                                        center=[0.0, 0.0, 3.0], sigma=[0.3, 0.3, 0.6],
                                        sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the medium case, B to 1e-4, each slice's B passes started by the learned
+    # network (trained over the parameter-scan ranges, weights in the package)
+    "medium_learned": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=16, tol=1e-4, predict=3,
+                           dt=10.0,
+                           species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                           beams=[dict(np=[256, 256, 128], q=-1.0, m=1.0, gamma=20000.0,
+                                       peak_density=4.0, quiet_start=True,
+                                       center=[0.0, 0.0, 3.0], sigma=[0.3, 0.3, 0.6],
+                                       sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
     # the medium case with the reference's fixed 2 B passes per slice (no tolerance)
     "medium_fixed2": dict(grid=dict(ind=[9, 9, 9], box=BOX), iter=2, dt=10.0,
                           species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
@@ -187,6 +196,14 @@ def make_engine(qpgpu, cfg, device):
     sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False,
                            dt=cfg.get("dt", 0.0), tol=cfg.get("tol", 0.0),
                            predict=cfg.get("predict", False))
+    if cfg.get("predict") == 3:
+        w = os.path.join(ROOT, "quickpic-opensource_b200", "qpgpu", "predictor_weights.npy")
+        if not os.path.exists(w):
+            raise SystemExit(f"{w} is missing: train it with qpgpu/train_predictor.py")
+        net = qpgpu.Predictor(device=device)
+        net.set_params(np.load(w))
+        sim.set_predictor(net)
+        sim._net = net
     return ctx, sp, beams, sim
 
 
@@ -530,7 +547,9 @@ def sampled_slices(cfg, ctx, sp, sim, nsamples, threads):
     import oracle
 
     nx, ny, nz = ctx.nx, ctx.ny, ctx.nz
-    ocfg = dict(cfg, beams=[], store3d=False)
+    # the oracle starts each slice's passes from epw(j-1), the reference's start;
+    # under a tolerance the converged fields do not depend on the start
+    ocfg = dict(cfg, beams=[], store3d=False, predict=0)
     o32, o64 = oracle.Sim(ocfg, np.float32), oracle.Sim(ocfg, np.float64)
     samples = sorted({1 + ((2 * i + 1) * nz) // (2 * nsamples) for i in range(nsamples)})
     names = ("fxy", "psit", "bxy", "bz", "psi", "epw", "cu_k")
@@ -601,7 +620,9 @@ def workload_desc(cfg, name):
 
 def passes_desc(cfg):
     start = {1: ", started from the linear extrapolation of B_perp",
-             2: ", started from the quadratic extrapolation of B_perp"}.get(cfg.get("predict", 0), "")
+             2: ", started from the quadratic extrapolation of B_perp",
+             3: ", started by the learned network (BF16 tcgen05 convolutions)"}.get(
+        cfg.get("predict", 0), "")
     if cfg.get("tol", 0.0) > 0:
         return (f"B predictor-corrector passes per slice until the relative change of B_perp "
                 f"<= {cfg['tol']:g} (at most {cfg['iter']}){start}")
@@ -628,6 +649,7 @@ def run_reference(args, cfg):
     warm.close()
     c = dict(cfg)
     c["store3d"] = True  # the beam push reads the stored 3D fields
+    c["predict"] = 0  # the reference's start of the passes
     sim = oracle.Sim(c, np.float32)
     npl = int(sim.get("np")[0])
     nz = 1 << cfg["grid"]["ind"][2]

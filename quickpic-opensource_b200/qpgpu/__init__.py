@@ -723,6 +723,7 @@ class TrainingSet:
         h = C.c_void_p()
         _nn_check(lib().qp_nn_data_create(device, int(capacity), C.byref(h)))
         self.h = h
+        self.capacity = int(capacity)
 
     def __len__(self):
         return int(lib().qp_nn_data_count(self.h))
