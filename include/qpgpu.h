@@ -420,7 +420,8 @@ int qp_sim_profile(qp_sim* sim, int nslices, char* names, int names_len, double*
  * correction, per Fourier mode, of the quadratic extrapolation
  * 3 epw(j-1) - 3 epw(j-2) + epw(j-3), from epw(j-1) and the differences of
  * the three previous slices' B_perp, the current handed to the slice (cu_k)
- * and the mode coordinates.  It has no counterpart in the
+ * and the mode coordinates, for the modes kx, ky < 128 (the window it is
+ * trained on; the other modes start from the extrapolation alone).  It has no counterpart in the
  * reference, whose passes start from epw(j-1) (simulation_class.f03:676); it
  * replaces that start when qp_sim_desc.predict = 3, and the passes still run
  * to the tolerance.  Layer l: weights W[9][cin][cout] (tap = 3 dy + dx, dy and
@@ -460,7 +461,7 @@ typedef struct {
   unsigned long long seed; /* minibatch draws */
 } qp_nn_train_desc;
 typedef struct {
-  double first_loss, last_loss; /* minibatch loss at the first and the last step */
+  double first_loss, last_loss; /* mean minibatch loss of the first and the last tenth */
   double gpu_ms;                /* device time of the training */
   int steps;
   int reserved;

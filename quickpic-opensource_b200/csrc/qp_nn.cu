@@ -204,6 +204,17 @@ __device__ __forceinline__ float nn_base(float e1, float e0, float em) {
   return 3.f * (e1 - e0) + em;
 }
 
+// The network's correction of a mode, bounded: at most the size of the
+// extrapolation step itself plus 5 % of the mode, and 0 if it is not finite.
+// Out of its training distribution the network can then move the start only
+// within the neighbourhood the extrapolation already spans; the passes that
+// follow run to the tolerance from wherever the start is.
+__device__ __forceinline__ float nn_bounded(float d, float step, float e1) {
+  const float lim = fabsf(step) + 0.05f * fabsf(e1);
+  if (!(fabsf(d) <= 3.0e38f)) return 0.f;
+  return fminf(fmaxf(d, -lim), lim);
+}
+
 // ---------------------------------------------------------------- the kernels
 enum { EPI_RELU = 0, EPI_MASK = 1, EPI_F32 = 2, EPI_EPW = 3 };
 
@@ -385,8 +396,8 @@ __global__ void __launch_bounds__(128) k_conv3x3(const __grid_constant__ CUtenso
       a.pl.prev_y[o] = e1y;
       float px = nn_base(e1x, e0x, emx), py = nn_base(e1y, e0y, emy);
       if (kx >= 1 && ky >= 1) {  // the modes kx = 0, ky = 0 take the extrapolation alone
-        px += sB * (acc[0] + a.bias[0]);
-        py += sB * (acc[1] + a.bias[1]);
+        px += nn_bounded(sB * (acc[0] + a.bias[0]), px - e1x, e1x);
+        py += nn_bounded(sB * (acc[1] + a.bias[1]), py - e1y, e1y);
       }
       a.pl.epw_x[o] = px;
       a.pl.epw_y[o] = py;
@@ -401,12 +412,13 @@ __global__ void __launch_bounds__(128) k_conv3x3(const __grid_constant__ CUtenso
     if (mma_out) mbar_wait(&bar[2], (uint32_t)(k & 1));
     flag_error(a.err, 1);
   }
-  // EPI_EPW: the modes outside the conv image (kx = nx, or ky = ny) take the
-  // quadratic extrapolation
-  if (EPI == EPI_EPW && blockIdx.x == 0 && !*s_err) {
-    for (int i = tid; i < a.ny + 1 + a.nx; i += 128) {
-      const int kx = i <= a.ny ? a.nx : i - a.ny - 1;
-      const int ky = i <= a.ny ? i : a.ny;
+  // EPI_EPW: the modes outside the conv image (the network's low-mode window)
+  // take the quadratic extrapolation alone, spread over every CTA
+  if (EPI == EPI_EPW && !*s_err) {
+    const long long nm = (long long)(a.nx + 1) * (a.ny + 1);
+    for (long long i = (long long)blockIdx.x * 128 + tid; i < nm; i += (long long)gridDim.x * 128) {
+      const int kx = (int)(i / (a.ny + 1)), ky = (int)(i - (long long)kx * (a.ny + 1));
+      if (kx < a.H && ky < a.W) continue;
       const size_t o = (size_t)kx * a.kp + ky;
       const float e1x = a.pl.epw_x[o], e1y = a.pl.epw_y[o];
       const float e0x = a.pl.prev_x[o], e0y = a.pl.prev_y[o];
@@ -674,6 +686,7 @@ __device__ __forceinline__ void nn_feature(const NNSlicePlanes& p, size_t o, int
   f[8] = safe_div(p.cu_z[o], sc[2]);
   f[9] = (float)kx / (float)nx;
   f[10] = (float)ky / (float)ny;
+  f[11] = p.dxi * 25.6f;
   for (int i = NN_FEATURES; i < 16; ++i) f[i] = 0.f;
   g0->x = pack_bf16(f[0], f[1]);
   g0->y = pack_bf16(f[2], f[3]);
@@ -685,16 +698,17 @@ __device__ __forceinline__ void nn_feature(const NNSlicePlanes& p, size_t o, int
   g1->w = pack_bf16(f[14], f[15]);
 }
 
-// inference: the input image [2][1][nx][ny][8] of the slice; scale_out = epw scale
-__global__ void k_nn_features(NNSlicePlanes p, int nx, int ny, int kp, const float* part,
-                              __nv_bfloat16* img, float* scale_out) {
+// inference: the input image [2][1][hc][wc][8] of the slice's low-mode
+// window kx < hc, ky < wc; scale_out = the epw scale
+__global__ void k_nn_features(NNSlicePlanes p, int nx, int ny, int kp, int hc, int wc,
+                              const float* part, __nv_bfloat16* img, float* scale_out) {
   __shared__ float sc[3];
   nn_scales(part, nx, ny, sc);
   if (blockIdx.x == 0 && threadIdx.x == 0) scale_out[0] = sc[0];
-  const long long n = (long long)nx * ny;
+  const long long n = (long long)hc * wc;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int kx = (int)(i / ny), ky = (int)(i - (long long)kx * ny);
+    const int kx = (int)(i / wc), ky = (int)(i - (long long)kx * wc);
     const size_t o = (size_t)kx * kp + ky;
     uint4 g0, g1;
     nn_feature(p, o, kx, ky, nx, ny, sc, p.epw_x[o], p.epw_y[o], p.prev_x[o], p.prev_y[o],
@@ -981,8 +995,9 @@ struct qp_nn_data {
 namespace qp {
 struct NNRuntime {
   int nx = 0, ny = 0, kp = 0;
-  __nv_bfloat16* img = nullptr;   // [2][1][nx][ny][8]
-  __nv_bfloat16* act[2] = {};     // [4][1][nx][ny][8]
+  int hc = 0, wc = 0;             // the low-mode window the network corrects
+  __nv_bfloat16* img = nullptr;   // [2][1][hc][wc][8]
+  __nv_bfloat16* act[2] = {};     // [4][1][hc][wc][8]
   float* part = nullptr;          // norm partials
   float* scale = nullptr;         // the slice's epw scale
   CUtensorMap m_img, m_act[2];
@@ -1440,7 +1455,11 @@ extern "C" int qp_nn_train(qp_nn* nn, qp_nn_data* t, const qp_nn_train_desc* d,
   cudaEventRecord(e0, s);
   const float inv_n = 1.f / (2.f * (float)B * H * W);
   const float b1 = 0.9f, b2 = 0.999f;
-  std::vector<float> losses;
+  // every step's minibatch loss, kept on the device and read once at the end
+  float* hist = nullptr;
+  if (!rc && (cudaMalloc(&hist, sizeof(float) * d->steps) != cudaSuccess ||
+              cudaMemsetAsync(hist, 0, sizeof(float) * d->steps, s) != cudaSuccess))
+    rc = nn_fail(__LINE__, "out of device memory (training buffers)");
   for (int it = 0; it < d->steps && !rc; ++it) {
     k_nn_gather<<<dim3(32, B), 256, 0, s>>>(t->d, idx + (size_t)it * B, bt);
     // the learning rate steps down to 0.3 and 0.1 of its start at 1/2 and 3/4 of the run
@@ -1448,9 +1467,8 @@ extern "C" int qp_nn_train(qp_nn* nn, qp_nn_data* t, const qp_nn_train_desc* d,
     rc = nn_forward(nn, m_in, 0, wk.act, wk.act_halo, B, H, W, wk.out32, nullptr, nullptr, 0, 0,
                     0, s);
     if (rc) break;
-    cudaMemsetAsync(nn->loss, 0, sizeof(float), s);
     cudaMemsetAsync(nn->grad, 0, sizeof(float) * nn->nparams, s);
-    k_nn_loss<<<256, 256, 0, s>>>(wk.out32, bt, 0, B, H, W, inv_n, wk.dy5, nn->loss);
+    k_nn_loss<<<256, 256, 0, s>>>(wk.out32, bt, 0, B, H, W, inv_n, wk.dy5, hist + it);
     rc = nn_backward(nn, m_in, 0, wk.act, wk.act_halo, wk.dy5, wk.dy5_tile, wk.dy5_halo, wk.dx,
                      wk.dx_tile, wk.dx_halo, B, H, W, s);
     if (rc) break;
@@ -1460,13 +1478,11 @@ extern "C" int qp_nn_train(qp_nn* nn, qp_nn_data* t, const qp_nn_train_desc* d,
     k_nn_adam<<<64, 256, 0, s>>>(nn->master, nn->grad, nn->m, nn->v, nn->nparams, lr, b1, b2, c1,
                                  c2, 1e-8f);
     rc = nn_pack(nn, s);
-    if (!rc && (it == 0 || it == d->steps - 1 || (it + 1) % 100 == 0)) {
-      float l = 0.f;
-      cudaMemcpyAsync(&l, nn->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
-      if (cudaStreamSynchronize(s) != cudaSuccess) rc = nn_fail(__LINE__, "training step failed");
-      losses.push_back(l);
-    }
   }
+  std::vector<float> losses(d->steps, 0.f);
+  if (!rc && cudaMemcpyAsync(losses.data(), hist, sizeof(float) * d->steps,
+                             cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = nn_fail(__LINE__, "training loss download failed");
   cudaEventRecord(e1, s);
   if (!rc) rc = nn_check_err(nn, s);
   float ms = 0.f;
@@ -1482,9 +1498,17 @@ extern "C" int qp_nn_train(qp_nn* nn, qp_nn_data* t, const qp_nn_train_desc* d,
   cudaFree(bt.target);
   cudaFree(bt.scale);
   cudaFree(idx);
+  cudaFree(hist);
   if (!rc && st) {
-    st->first_loss = losses.empty() ? 0.0 : losses.front();
-    st->last_loss = losses.empty() ? 0.0 : losses.back();
+    // the mean minibatch loss over the first and over the last tenth of the run
+    const int w = std::max(1, d->steps / 10);
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < w; ++i) {
+      a += losses[i];
+      b += losses[d->steps - 1 - i];
+    }
+    st->first_loss = a / w;
+    st->last_loss = b / w;
     st->gpu_ms = ms;
     st->steps = d->steps;
   }
@@ -1497,20 +1521,25 @@ namespace qp {
 int nn_runtime_create(const GridDims& g, NNRuntime** out) {
   if (g.ny % TM != 0 || g.nx < 2)
     return nn_fail(__LINE__, "learned predictor: ny must be a multiple of 128");
+  static_assert(NN_CROP == TM, "the network's window is one tile wide");
   if (!encode_fn()) return nn_fail(__LINE__, "cuTensorMapEncodeTiled is not available");
   NNRuntime* r = new NNRuntime();
   r->nx = g.nx;
   r->ny = g.ny;
   r->kp = g.kp;
-  const size_t px = (size_t)g.nx * g.ny;
+  // the network corrects the modes it was trained on, kx, ky < 128 (the
+  // training crop); the others take the quadratic extrapolation
+  r->hc = std::min(g.nx, NN_CROP);
+  r->wc = NN_CROP;
+  const size_t px = (size_t)r->hc * r->wc;
   bool ok = cudaMalloc(&r->img, px * NN_CIN0 * 2) == cudaSuccess &&
             cudaMalloc(&r->act[0], px * NN_CH * 2) == cudaSuccess &&
             cudaMalloc(&r->act[1], px * NN_CH * 2) == cudaSuccess &&
             cudaMalloc(&r->part, sizeof(float) * 3 * NN_NORM_BLOCKS) == cudaSuccess &&
             cudaMalloc(&r->scale, sizeof(float)) == cudaSuccess;
-  ok = ok && !halo_map(&r->m_img, r->img, NN_CIN0 / 8, 1, g.nx, g.ny) &&
-       !halo_map(&r->m_act[0], r->act[0], NN_CH / 8, 1, g.nx, g.ny) &&
-       !halo_map(&r->m_act[1], r->act[1], NN_CH / 8, 1, g.nx, g.ny);
+  ok = ok && !halo_map(&r->m_img, r->img, NN_CIN0 / 8, 1, r->hc, r->wc) &&
+       !halo_map(&r->m_act[0], r->act[0], NN_CH / 8, 1, r->hc, r->wc) &&
+       !halo_map(&r->m_act[1], r->act[1], NN_CH / 8, 1, r->hc, r->wc);
   if (!ok) {
     nn_runtime_destroy(r);
     return nn_fail(__LINE__, "learned predictor set-up failed");
@@ -1531,13 +1560,13 @@ int nn_predict(NNRuntime* r, const void* net, const NNSlicePlanes& p, const Grid
                DevStatus* st, cudaStream_t s) {
   qp_nn* nn = const_cast<qp_nn*>(static_cast<const qp_nn*>(net));
   k_nn_norms<<<NN_NORM_BLOCKS, 256, 0, s>>>(p, g.nx, g.ny, g.kp, r->part);
-  k_nn_features<<<NN_NORM_BLOCKS * 4, 256, 0, s>>>(p, g.nx, g.ny, g.kp, r->part, r->img,
-                                                    r->scale);
+  k_nn_features<<<NN_NORM_BLOCKS, 256, 0, s>>>(p, g.nx, g.ny, g.kp, r->hc, r->wc, r->part,
+                                                r->img, r->scale);
   // layers 1-4 ping-pong between the two activation buffers; every layer's
   // input is the previous output, so the four maps cycle through them
   __nv_bfloat16* act[4] = {r->act[0], r->act[1], r->act[0], r->act[1]};
   const CUtensorMap amap[4] = {r->m_act[0], r->m_act[1], r->m_act[0], r->m_act[1]};
-  if (nn_forward(nn, r->m_img, 0, act, amap, 1, g.nx, g.ny, nullptr, &p, r->scale, g.kp, g.nx,
+  if (nn_forward(nn, r->m_img, 0, act, amap, 1, r->hc, r->wc, nullptr, &p, r->scale, g.kp, g.nx,
                  g.ny, s))
     return -1;
   (void)st;

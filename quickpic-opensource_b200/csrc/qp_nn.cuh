@@ -4,7 +4,8 @@
 // The predictor maps, for slice j, the Fourier-space B_perp iterates of the
 // three previous slices (epw(j-1), epw(j-2), epw(j-3)), the current handed to slice j
 // (cu_k after the xi extrapolation) and the mode coordinates to a correction
-// of the quadratic extrapolation 3 epw(j-1) - 3 epw(j-2) + epw(j-3): the start of slice j's
+// of the quadratic extrapolation 3 epw(j-1) - 3 epw(j-2) + epw(j-3), in the
+// low-mode window kx, ky < 128 it is trained on: the start of slice j's
 // predictor-corrector passes (the hook at simulation_class.f03:676, where the
 // reference starts from epw(j-1)).  The passes still run to the tolerance.
 //
@@ -12,7 +13,7 @@
 // channels / 8): 8 channels of one pixel are 16 contiguous bytes, which is one
 // row of a tcgen05 core matrix, so a 3x3 tap of the convolution is the same
 // shared-memory tile addressed from another start (an implicit GEMM with no
-// im2col copy).  H runs over kx (0..nx-1), W over ky (0..ny-1).
+// im2col copy).  H runs over kx, W over ky, from mode 0.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -27,10 +28,11 @@ constexpr int NN_CH = 32;       // hidden channels
 constexpr int NN_NLAST = 16;    // output channels of layer 5 as computed (NN_OUT used)
 constexpr int NN_OUT = 2;       // the correction of epw_x, epw_y
 // e1, e1 - e0, e0 - e(-1) (x and y each, over the epw scale), cu.x, cu.y, cu.z
-// (over their scales), kx/nx, ky/ny: the history enters as differences, so
-// that the network sees slopes and curvatures without the cancellation of
-// nearly equal bfloat16 values
-constexpr int NN_FEATURES = 11;
+// (over their scales), kx/nx, ky/ny, the slice width dxi / (10/256): the
+// history enters as differences, so that the network sees slopes and
+// curvatures without the cancellation of nearly equal bfloat16 values, and
+// the slice width sets how far the fields move from one slice to the next
+constexpr int NN_FEATURES = 12;
 constexpr int NN_CROP = 128;    // side of the training crop (the low-mode corner)
 constexpr int NN_NORM_BLOCKS = 148;
 
@@ -51,6 +53,7 @@ struct NNSlicePlanes {
   const float* cu_x;     // the current handed to slice j
   const float* cu_y;
   const float* cu_z;
+  float dxi;             // slice width (c/wp)
 };
 
 struct NNRuntime;  // per-simulation buffers and tensor maps (qp_nn.cu)

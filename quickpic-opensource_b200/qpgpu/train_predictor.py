@@ -9,11 +9,14 @@ held-out simulations: passes per slice from the carried start, the quadratic
 extrapolation and the learned start, at the same tolerance.
 
 Ranges (the batched parameter scan's): transverse grids 128^2, 256^2, 512^2
-drawn log-uniform, 256 slices over a 12 x 12 x 10 c/wp box, 2 x 2 particles per
-cell, tri-Gaussian beam with nb/np log-uniform in [0.5, 20] and sigma_r uniform
-in [0.1, 0.5] c/wp (a pair with (nb/np) sigma_r^2 > 1, a full blow-out, is drawn
-again), sigma_z = 0.5 c/wp, beam particles in proportion to the grid area
-(262,144 at 128^2, at most 2,097,152), gamma = 20000.
+drawn log-uniform, 2 x 2 particles per cell, tri-Gaussian beam with nb/np
+log-uniform in [0.5, 20] and sigma_r uniform in [0.1, 0.5] c/wp (a pair with
+(nb/np) sigma_r^2 > 1, a full blow-out, is drawn again), beam particles in
+proportion to the grid area (262,144 at 128^2, at most 2,097,152), gamma =
+20000, over a 12 x 12 x 10 c/wp box.  The scan's 256 slices and sigma_z = 0.5
+c/wp are widened to 256 or 512 slices and sigma_z uniform in [0.4, 0.7] c/wp,
+so that the slice width (a feature of the network) and the bunch length of the
+512-slice medium case are inside the training set.
 
     python quickpic-opensource_b200/qpgpu/train_predictor.py --pairs 20000 \
         --out quickpic-opensource_b200/qpgpu/predictor_weights.npy
@@ -46,16 +49,19 @@ def draw_instances(n, seed):
             if peak * sr * sr <= 1.0:
                 break
         nb = {7: [64, 64, 64], 8: [128, 128, 64], 9: [128, 128, 128]}[ind]
-        out.append(dict(ind=ind, peak=peak, sigma_r=sr, np=nb))
+        nz_ind = int(rng.integers(8, 10))
+        sz = float(rng.uniform(0.4, 0.7))
+        out.append(dict(ind=ind, peak=peak, sigma_r=sr, sigma_z=sz, nz_ind=nz_ind, np=nb))
     return out
 
 
-def make_sim(inst, predict=0, tol=1e-4, iter=16, nz_ind=8, device=0):
-    c = qpgpu.Context(inst["ind"], inst["ind"], nz_ind, BOX, device=device)
+def make_sim(inst, predict=0, tol=1e-4, iter=16, device=0):
+    c = qpgpu.Context(inst["ind"], inst["ind"], inst["nz_ind"], BOX, device=device)
     sp = qpgpu.Species2d(c, ppc=(2, 2))
     bm = qpgpu.Beam3d(c, inst["np"], q=-1.0, m=1.0, gamma=20000.0, peak_density=inst["peak"],
                       quiet_start=True, center=[0.0, 0.0, 2.5],
-                      sigma=[inst["sigma_r"], inst["sigma_r"], 0.5], sigma_v=[0.0, 0.0, 0.0])
+                      sigma=[inst["sigma_r"], inst["sigma_r"], inst["sigma_z"]],
+                      sigma_v=[0.0, 0.0, 0.0])
     sim = qpgpu.Simulation(c, [sp], [bm], iter=iter, store3d=False, tol=tol, predict=predict)
     return c, sp, bm, sim
 
@@ -116,7 +122,7 @@ def main():
     ap.add_argument("--eval", type=int, default=6, help="held-out simulations")
     ap.add_argument("--out", default=os.path.join(HERE, "predictor_weights.npy"))
     args = ap.parse_args()
-    per = 256
+    per = 384  # slices per instance, on average
     n_inst = (args.pairs + per - 1) // per
     t0 = time.time()
     data = qpgpu.TrainingSet(args.pairs)

@@ -109,7 +109,8 @@ def test_recording_and_training(qp):
     kx = np.arange(128)[:, None] / 128.0
     ky = np.arange(128)[None, :] / 128.0
     assert np.abs(img[9] - kx).max() < 4e-3 and np.abs(img[10] - ky).max() < 4e-3
-    assert np.all(img[11:] == 0)
+    assert np.abs(img[11] - (10.0 / 32) * 25.6).max() < 2e-2  # the slice width
+    assert np.all(img[12:] == 0)
     assert sc > 0 and np.isfinite(tgt).all()
     net = qp.Predictor(seed=3)
     st = net.train(data, steps=300, batch=8, lr=2e-3, seed=1)
