@@ -295,6 +295,16 @@ int qp_beam_download(qp_beam* b, float* part /* (7, np) */);
  * particles, part3d%rrst (part3d_class.f03:315-331), without the HDF5 file. */
 int qp_beam_upload(qp_beam* b, const float* part, long long np);
 int qp_beam_download_q3d(qp_beam* b, float* rf /* (nx+2, ny+1, nz+1) */);
+/* Beam restart (beam3d%wrst / %rrst, beam3d_class.f03:220-290 -> hdf5io
+ * wpart / rpart, hdf5io_class.f03:1301-1422) in the reference's path layout
+ * dir/RST/Beam-NNNN/RST-beamNNNN-RRRRRRRRRR_SSSSSSSS (beam from 1, rank,
+ * dump step; simulation_class.f03:1261-1277) with the reference's content,
+ * the particle count tp and part(7, tp).  The HDF5 container is not built
+ * (no HDF5 library in this build): the file ends in .qprst and holds
+ * "QPRST001", tp (int64) and part(7, tp) (float32, column-major).  read
+ * replaces the beam's particles (tp must fit its capacity). */
+int qp_beam_write_restart(qp_beam* b, const char* dir, int beam, int rank, int step);
+int qp_beam_read_restart(qp_beam* b, const char* dir, int beam, int rank, int step);
 
 /* ----------------------------------------------------- fused 3D step */
 

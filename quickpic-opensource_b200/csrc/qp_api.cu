@@ -1313,5 +1313,69 @@ extern "C" int qp_beam_download_q3d(qp_beam* b, float* rf) {
   return 0;
 }
 
+// ---------------------------------------------------------------- beam restart
+// The reference writes a beam's restart (beam3d%wrst -> part3d%wrst ->
+// hdf5io wpart, hdf5io_class.f03:1301-1360) as
+//   ./RST/Beam-NNNN/RST-beamNNNN-RRRRRRRRRR_SSSSSSSS.h5
+// (beam NNNN from 1, rank R, dump S; simulation_class.f03:1261-1277) holding
+// the root attribute tp = particle count and one dataset named
+// RST-beamNNNN-RRRRRRRRRR with part(7, tp).  This build has no HDF5 library,
+// so the same path carries the suffix .qprst instead of .h5 and the same
+// content in a flat container: the 8 bytes "QPRST001", tp as a little-endian
+// int64, then part(7, tp) as float32, column-major.
+static std::string restart_path(const char* dir, int beam, int rank, int step) {
+  char tail[96];
+  std::snprintf(tail, sizeof(tail), "RST/Beam-%04d/RST-beam%04d-%010d_%08d.qprst", beam, beam,
+                rank, step);
+  std::string d = dir && dir[0] ? std::string(dir) : std::string(".");
+  if (d.back() != '/') d += '/';
+  return d + tail;
+}
+
+extern "C" int qp_beam_write_restart(qp_beam* b, const char* dir, int beam, int rank, int step) {
+  if (!b) return fail(nullptr, __LINE__, "null beam");
+  qp_ctx* ctx = b->ctx;
+  if (beam < 1 || beam > 9999 || rank < 0 || step < 0 || step > 99999999)
+    return fail(ctx, __LINE__, "restart: beam 1..9999, rank >= 0, step 0..99999999");
+  const std::string path = restart_path(dir, beam, rank, step);
+  const std::string folder = path.substr(0, path.rfind('/'));
+  const std::string mk = "mkdir -p '" + folder + "'";
+  if (folder.find('\'') != std::string::npos || std::system(mk.c_str()) != 0)
+    return fail(ctx, __LINE__, "restart: cannot create " + folder);
+  const long long np = b->b.np;
+  std::vector<float> part((size_t)7 * np);
+  if (np > 0 && qp_beam_download(b, part.data())) return -1;
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return fail(ctx, __LINE__, "restart: cannot write " + path);
+  const long long tp = np;
+  bool ok = std::fwrite("QPRST001", 1, 8, f) == 8 && std::fwrite(&tp, 8, 1, f) == 1 &&
+            (np == 0 || std::fwrite(part.data(), sizeof(float), part.size(), f) == part.size());
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(ctx, __LINE__, "restart: short write to " + path);
+  return 0;
+}
+
+extern "C" int qp_beam_read_restart(qp_beam* b, const char* dir, int beam, int rank, int step) {
+  if (!b) return fail(nullptr, __LINE__, "null beam");
+  qp_ctx* ctx = b->ctx;
+  const std::string path = restart_path(dir, beam, rank, step);
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return fail(ctx, __LINE__, "restart: cannot open " + path);
+  char magic[8];
+  long long tp = -1;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "QPRST001", 8) == 0 &&
+            std::fread(&tp, 8, 1, f) == 1 && tp >= 0 && tp <= b->cap;
+  std::vector<float> part;
+  if (ok) {
+    part.resize((size_t)7 * tp);
+    ok = tp == 0 || std::fread(part.data(), sizeof(float), part.size(), f) == part.size();
+  }
+  std::fclose(f);
+  if (!ok) return fail(ctx, __LINE__, "restart: " + path + " is not a beam restart of this beam");
+  if (qp_beam_upload(b, part.data(), tp)) return -1;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
 #include "qp_sim.inc"
 #include "qp_scan.inc"

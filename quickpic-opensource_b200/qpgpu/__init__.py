@@ -468,6 +468,14 @@ class Beam3d:
         self.ctx._check(self.ctx._L.qp_beam_upload(self.h, _ptr(part),
                                                    C.c_longlong(part.shape[1])))
 
+    def write_restart(self, dir, beam=1, rank=0, step=0):
+        """beam3d%wrst: dir/RST/Beam-NNNN/RST-beamNNNN-RRRRRRRRRR_SSSSSSSS.qprst"""
+        self.ctx._check(self.ctx._L.qp_beam_write_restart(self.h, dir.encode(), beam, rank, step))
+
+    def read_restart(self, dir, beam=1, rank=0, step=0):
+        """beam3d%rrst: replaces the particles with the restart file's."""
+        self.ctx._check(self.ctx._L.qp_beam_read_restart(self.h, dir.encode(), beam, rank, step))
+
     def get_q3d(self):
         c = self.ctx
         out = np.zeros((c.nx + 2, c.ny + 1, c.nz + 1), dtype=np.float32, order="F")

