@@ -722,13 +722,35 @@ static int species_profile(qp_ctx* ctx, const qp_species_desc* d, PlasmaProfile*
 // Loads the species' profile at s (PPDBLKP2L: particles per tile and nppmx;
 // PPPMOVIN2L: a stable copy into the tiles) into the pristine buffer P0 and
 // the live buffer A, growing the buffers when the load needs more room.
+// species2d%renew at s (species2d_class.f03:138-164 -> part2d%renew,
+// part2d_class.f03:226-254): the particles of the profile, which depend on s
+// only through the longitudinal density factor, come from the pristine copy
+// on the device, with charge qm(s) * (transverse factor): no host reload.
+static int species_renew_device(qp_species* sp, float s) {
+  qp_ctx* ctx = sp->ctx;
+  const TileGeom& tg = ctx->tg;
+  float qm = 0.f;
+  std::string err;
+  if (!plasma_qm(sp->prof, s, &qm, &err)) return fail(ctx, __LINE__, "plasma loader: " + err);
+  if (sp->A.cap < sp->P0.cap) return fail(ctx, __LINE__, "renew: capacity shrank");
+  const long long n = (long long)tg.ntiles * sp->A.cap;
+  for (int k = 0; k < NCOMP; ++k)
+    launch_lin(n, sp->A.c[k], nullptr, nullptr, 0.f, LIN_FILL, ctx->st, ctx->stream);
+  if (part_copy(ctx, sp->A, sp->P0)) return -1;
+  launch_lin(n, sp->A.c[7], sp->A.c[7], nullptr, qm, LIN_SCALE, ctx->st, ctx->stream);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 static int species_load(qp_species* sp, float s) {
   qp_ctx* ctx = sp->ctx;
   const GridDims& g = ctx->g;
   const TileGeom& tg = ctx->tg;
   std::vector<float> c[8];
   std::string err;
-  const long long np = plasma_load(sp->prof, g.nx, g.ny, s, c, &err);
+  // the pristine copy holds each particle's transverse charge factor; renew
+  // multiplies it by the longitudinal qm(s) on the device
+  const long long np = plasma_load(sp->prof, g.nx, g.ny, s, true, c, &err);
   if (np < 0) return fail(ctx, __LINE__, "plasma loader: " + err);
   sp->np = np;
   std::vector<int> cnt(tg.ntiles, 0), tile(np);
@@ -771,10 +793,7 @@ static int species_load(qp_species* sp, float s) {
     CK(cudaMemcpy(sp->P0.c[k], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
   }
   CK(cudaMemcpy(sp->P0.count, cnt.data(), sizeof(int) * tg.ntiles, cudaMemcpyHostToDevice));
-  for (int k = 0; k < NCOMP; ++k)
-    launch_lin((long long)tg.ntiles * sp->A.cap, sp->A.c[k], nullptr, nullptr, 0.f, LIN_FILL,
-               ctx->st, ctx->stream);
-  return part_copy(ctx, sp->A, sp->P0);
+  return species_renew_device(sp, s);
 }
 
 extern "C" int qp_species_create(qp_ctx* ctx, const qp_species_desc* d, float s,
@@ -837,17 +856,7 @@ extern "C" int qp_species_destroy(qp_species* sp) {
 // afresh at s (species2d%renew, species2d_class.f03:138-164).
 extern "C" int qp_species_renew(qp_species* sp, float s) {
   qp_ctx* ctx = sp->ctx;
-  if (!sp->prof.fs.empty()) {
-    if (species_load(sp, s) || species_background(sp)) return -1;
-    CK(cudaStreamSynchronize(ctx->stream));
-    return 0;
-  }
-  if (sp->A.cap < sp->P0.cap) return fail(ctx, __LINE__, "renew: capacity shrank");
-  for (int c = 0; c < NCOMP; ++c)
-    launch_lin((long long)ctx->tg.ntiles * sp->A.cap, sp->A.c[c], nullptr, nullptr, 0.f, LIN_FILL,
-               ctx->st, ctx->stream);
-  if (part_copy(ctx, sp->A, sp->P0)) return -1;
-  if (species_background(sp)) return -1;
+  if (species_renew_device(sp, s) || species_background(sp)) return -1;
   CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }

@@ -127,11 +127,18 @@ static bool longitudinal(const PlasmaProfile& p, float s, float* den, std::strin
   return true;
 }
 
-long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s,
-                      std::vector<float> (&c)[8], std::string* err) {
+bool plasma_qm(const PlasmaProfile& p, float s, float* qm, std::string* err) {
   float den_temp;
-  if (!longitudinal(p, s, &den_temp, err)) return -1;
-  const float qm = den_temp * p.den * p.q / std::fabs(p.q) / (float)p.xppc / (float)p.yppc;
+  if (!longitudinal(p, s, &den_temp, err)) return false;
+  *qm = den_temp * p.den * p.q / std::fabs(p.q) / (float)p.xppc / (float)p.yppc;
+  return true;
+}
+
+long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s, bool factor_only,
+                      std::vector<float> (&c)[8], std::string* err) {
+  float den_temp, qm_s;
+  if (!longitudinal(p, s, &den_temp, err) || !plasma_qm(p, s, &qm_s, err)) return -1;
+  const float qm = factor_only ? 1.0f : qm_s;
   const int nr = (int)p.r.size();
   if (p.profile == 12) {
     if (nr < 2 || (int)p.fr.size() != nr) {

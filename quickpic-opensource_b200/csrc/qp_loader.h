@@ -32,10 +32,18 @@ struct PlasmaProfile {
   std::vector<float> s, fs;                         // longitudinal piecewise
 };
 
+// The charge per particle of profile p before its transverse factor, at
+// propagation distance s: den_temp(s) * den * sign(q) / (xppc * yppc)
+// (dist2d_0xx, fdist2d_class.f03:246-248 with 421-438).  false with *err on a
+// bad longitudinal profile.
+bool plasma_qm(const PlasmaProfile& p, float s, float* qm, std::string* err);
+
 // Loads profile p at propagation distance s (dist2d_0xx for one rank:
 // cells i = 2..nx-1, j = 2..ny, order i, j, ix, iy).  Returns the number of
-// particles, or -1 with a message in *err.
-long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s,
+// particles, or -1 with a message in *err.  With factor_only, c[7] holds the
+// transverse factor of each particle's charge (1, or the profile's weight)
+// and the charge is qm(s) * c[7], the same single product the loader forms.
+long long plasma_load(const PlasmaProfile& p, int nx, int ny, float s, bool factor_only,
                       std::vector<float> (&c)[8], std::string* err);
 
 // One beam's loader parameters with lengths in cells (the init_fdist3d_0xx
