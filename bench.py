@@ -89,6 +89,18 @@ CONFIGS = {
                                     peak_density=4.0, quiet_start=True, center=[0.0, 0.0, 3.0],
                                     sigma=[0.3, 0.3, 0.6],
                                     sigma_v=[0.01 / 0.3, 0.01 / 0.3, 200.0])]),
+    # the nonlinear blow-out case: 1024^2 x 1024 slices, 2x2 ppc (4.2M
+    # electrons), a narrow drive beam (sigma_r 0.1, sigma_z 0.4, nb/np 20,
+    # 16.8M particles) and a witness bunch 4 c/wp behind it (nb/np 10, 2.1M
+    # particles, the drive's sigmas), B to 1e-4
+    "blowout": dict(grid=dict(ind=[10, 10, 10], box=BOX), iter=16, tol=1e-4, dt=10.0,
+                    species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
+                    beams=[dict(np=[256, 256, 256], q=-1.0, m=1.0, gamma=20000.0,
+                                peak_density=20.0, quiet_start=True, center=[0.0, 0.0, 2.0],
+                                sigma=[0.1, 0.1, 0.4], sigma_v=[0.0, 0.0, 0.0]),
+                           dict(np=[128, 128, 128], q=-1.0, m=1.0, gamma=20000.0,
+                                peak_density=10.0, quiet_start=True, center=[0.0, 0.0, 6.0],
+                                sigma=[0.1, 0.1, 0.4], sigma_v=[0.0, 0.0, 0.0])]),
     # the small CPU-runnable case (128^3, 2x2 ppc, 262,144 beam particles)
     "small": dict(grid=dict(ind=[7, 7, 7], box=BOX), iter=2, dt=10.0,
                   species=dict(ppc=[2, 2], q=-1.0, m=1.0, density=1.0, xtras=0.2),
@@ -611,11 +623,13 @@ def sampled_slices(cfg, ctx, sp, sim, nsamples, threads):
 
 def workload_desc(cfg, name):
     g = cfg["grid"]["ind"]
-    b = cfg["beams"][0]
+    beams = "; ".join(
+        f"beam {int(np.prod(b['np']))} particles sigma_r={b['sigma'][0]} "
+        f"sigma_z={b['sigma'][2]} nb/np={b['peak_density']} at z={b['center'][2]}"
+        for b in cfg["beams"])
     return (f"{name}: {1 << g[0]}x{1 << g[1]} transverse, {1 << g[2]} slices, "
-            f"{cfg['species']['ppc'][0]}x{cfg['species']['ppc'][1]} ppc, beam "
-            f"{int(np.prod(b['np']))} particles sigma_r={b['sigma'][0]} sigma_z={b['sigma'][2]} "
-            f"nb/np={b['peak_density']}, {passes_desc(cfg)}, beam push dt={cfg.get('dt', 0.0)}")
+            f"{cfg['species']['ppc'][0]}x{cfg['species']['ppc'][1]} ppc, {beams}, "
+            f"{passes_desc(cfg)}, beam push dt={cfg.get('dt', 0.0)}")
 
 
 def passes_desc(cfg):
