@@ -492,6 +492,36 @@ def run_particle_case(args, cfg):
     ctx.close()
 
 
+def run_nn_train_case(args):
+    """Kernel case: training steps of the learned B start on pairs recorded
+    from one 3D step of a 128^2 x 128-slice case (passes to 1e-4); one step =
+    one Adam step on a minibatch of 32 pairs of 128 x 128 Fourier-mode images
+    (the 5 forward, 4 data-gradient and 5 weight-gradient tensor-core kernels).
+    FLOPs per step: 3 x 2 x MACs of the forward (the backward is twice the
+    forward)."""
+    import qpgpu
+
+    c = qpgpu.Context(7, 7, 7, BOX)
+    sp = qpgpu.Species2d(c, ppc=(2, 2))
+    bm = qpgpu.Beam3d(c, [64, 64, 64], q=-1.0, m=1.0, gamma=20000.0, peak_density=3.0,
+                      quiet_start=True, center=[0.0, 0.0, 2.5], sigma=[0.3, 0.3, 0.5])
+    sim = qpgpu.Simulation(c, [sp], [bm], iter=16, tol=1e-4, store3d=False)
+    data = qpgpu.TrainingSet(128)
+    sim.record(data)
+    sim.step3d()
+    net = qpgpu.Predictor(seed=1)
+    net.train(data, steps=max(1, args.warmup), batch=32, lr=1e-3)
+    st = net.train(data, steps=args.steps, batch=32, lr=1e-3)
+    macs_px = 9 * (16 * 32 + 3 * 32 * 32 + 32 * 16)
+    flops = 3 * 2 * macs_px * 32 * 128 * 128 * args.steps
+    print(json.dumps({"case": "nn_train", "steps": args.steps, "batch": 32,
+                      "image": [128, 128], "ms_per_step": st.gpu_ms / args.steps,
+                      "tflops": flops / (st.gpu_ms * 1e-3) / 1e12,
+                      "first_loss": st.first_loss, "last_loss": st.last_loss}), flush=True)
+    for o in (net, data, sim, bm, sp, c):
+        o.close()
+
+
 def _reduce(v, dist, op):
     if dist is None:
         return v
@@ -706,10 +736,12 @@ def main():
                     help="slices of one step checked against the FP64 oracle (and timed on "
                     "the FP32 oracle for the CPU baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="step", choices=["step", "fft", "amjdp", "push", "scan"],
+    ap.add_argument("--case", default="step",
+                    choices=["step", "fft", "amjdp", "push", "scan", "nn_train"],
                     help="step: the 3D step (the benchmark); fft: transform kernels alone; "
                     "amjdp / push: one particle routine alone; scan: the batched "
-                    "parameter scan (--scan-n instances)")
+                    "parameter scan (--scan-n instances); nn_train: training steps of the "
+                    "learned B start (the tensor-core kernels alone)")
     ap.add_argument("--scan-n", type=int, default=64)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
@@ -721,6 +753,9 @@ def main():
         return
     if args.case in ("amjdp", "push"):
         run_particle_case(args, cfg)
+        return
+    if args.case == "nn_train":
+        run_nn_train_case(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
