@@ -194,7 +194,7 @@ def ncu_traffic(kernel, workload):
     return None
 
 
-def make_engine(qpgpu, cfg, device):
+def make_engine(qpgpu, cfg, device, graphs=0):
     g = cfg["grid"]
     ctx = qpgpu.Context(g["ind"][0], g["ind"][1], g["ind"][2], g["box"], device=device)
     s = cfg["species"]
@@ -205,7 +205,8 @@ def make_engine(qpgpu, cfg, device):
         beams.append(qpgpu.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
                                   peak_density=b["peak_density"], quiet_start=b["quiet_start"],
                                   center=b["center"], sigma=b["sigma"], sigma_v=b["sigma_v"]))
-    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True, use_graphs=False,
+    sim = qpgpu.Simulation(ctx, [sp], beams, iter=cfg["iter"], store3d=True,
+                           use_graphs=bool(graphs),
                            dt=cfg.get("dt", 0.0), tol=cfg.get("tol", 0.0),
                            predict=cfg.get("predict", False))
     if cfg.get("predict") == 3:
@@ -222,7 +223,7 @@ def make_engine(qpgpu, cfg, device):
 def run_engine(args, cfg, rank, world, local_rank, dist):
     import qpgpu
 
-    ctx, sp, beams, sim = make_engine(qpgpu, cfg, local_rank)
+    ctx, sp, beams, sim = make_engine(qpgpu, cfg, local_rank, args.graphs)
     npl = sp.np()
     nz = ctx.nz
     for _ in range(args.warmup):
@@ -362,7 +363,8 @@ def run_scan_case(args):
         bm = qpgpu.Beam3d(ctx, b["np"], q=b["q"], m=b["m"], gamma=b["gamma"],
                           peak_density=b["peak_density"], quiet_start=True, center=b["center"],
                           sigma=b["sigma"], sigma_v=b["sigma_v"])
-        sim = qpgpu.Simulation(ctx, [sp], [bm], iter=cfg["iter"], store3d=False, dt=0.0)
+        sim = qpgpu.Simulation(ctx, [sp], [bm], iter=cfg["iter"], store3d=False, dt=0.0,
+                               use_graphs=bool(args.graphs))
         insts.append((ctx, sp, bm, sim))
     sims = [i[3] for i in insts]
     workers, _ = qpgpu.scan_tune(sims, probe_steps=1)
@@ -387,6 +389,7 @@ def run_scan_case(args):
             "config": {"workload": f"scan: {args.scan_n} instances, grids {grids}, 256 slices, "
                                    "2x2 ppc, iter=2, no beam push, 3D fields not kept",
                        "instances": args.scan_n, "workers": st.workers,
+                       "slice_graphs": bool(args.graphs),
                        "sequential_value": v_seq,
                        "speedup_vs_sequential": round(value / v_seq, 3),
                        "parallelism": "single"},
@@ -743,6 +746,8 @@ def main():
                     "parameter scan (--scan-n instances); nn_train: training steps of the "
                     "learned B start (the tensor-core kernels alone)")
     ap.add_argument("--scan-n", type=int, default=64)
+    ap.add_argument("--graphs", type=int, default=1, choices=[0, 1],
+                    help="1: each slice replayed from a captured CUDA graph (use_graphs)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.case == "scan":
@@ -797,6 +802,7 @@ def main():
                            "passes_per_slice": round(r["passes_per_slice"], 3),
                            "unconverged_slices": r["unconverged"],
                            "l2": "inputs larger than L2: each 3D step writes >4 GB of 3D fields",
+                           "slice_graphs": bool(args.graphs),
                            "parallelism": "replicas" if world > 1 else "single"},
                 "step_time_ms": r["t_ms"] / args.steps,
                 "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": cpu,

@@ -328,8 +328,13 @@ int qp_beam_read_restart(qp_beam* b, const char* dir, int beam, int rank, int st
  * vpot = 1 (with store3d = 1, one species) also keeps the vector potential
  * vpot3d of every slice (simulation_class.f03:711-716: field2d%vpot of the
  * last pass's current, fftkr, times -dex), downloaded as "vpot";
- * use_graphs is kept for binary compatibility and ignored: the slices are
- * launched directly;
+ * use_graphs = 1 captures a slice's launches as a CUDA graph, once per
+ * particle-buffer parity and number of passes enqueued, and replays it for
+ * every slice with the same two (a replay first checks every pointer and
+ * value the graph holds against the current ones and captures again when a
+ * buffer was grown or replaced); the results are the same as with direct
+ * launches; ignored with predict = 3, while recording, and in checked mode
+ * (QP_SYNC_CHECK=1);
  * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
  * step with beam3d%push of every beam with the stored bexyz, bbxyz
  * (simulation_class.f03:753-757), dt = 0 leaves the beams where they are. */
@@ -382,6 +387,9 @@ int qp_sim_begin3d(qp_sim* sim);
 int qp_sim_slices(qp_sim* sim, int n);
 int qp_sim_end3d(qp_sim* sim, qp_step_stats* stats);
 int qp_sim_next_slice(const qp_sim* sim);
+/* use_graphs: slice graphs captured so far (each capture follows a new pass
+ * count, parity or a replaced buffer; replays are not counted); -1 for NULL */
+int qp_sim_graph_captures(const qp_sim* sim);
 /* The Fourier-space fields a slice hands to the next, reference k-space
  * layout (dim, ny+1, nx+1): "epw" (transverse-B iterate, dim 2), "cu_k"
  * (current after the xi extrapolation, dim 3), and with predict > 0

@@ -535,6 +535,11 @@ class Simulation:
         """The slice the next slices() call starts with; 0 outside a step."""
         return int(self.ctx._L.qp_sim_next_slice(self.h))
 
+    @property
+    def graph_captures(self):
+        """With use_graphs: the slice graphs captured so far."""
+        return int(self.ctx._L.qp_sim_graph_captures(self.h))
+
     def set_field(self, name, arr):
         """Restore a field handed from slice to slice ("epw", "cu_k",
         "epw_prev", "epw_prev2"), reference k-space layout (dim, ny+1, nx+1)."""
