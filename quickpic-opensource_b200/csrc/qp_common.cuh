@@ -66,7 +66,7 @@ __host__ __device__ constexpr int lt_tw3(int P) { return 256 * P + 256; }  // fl
 __host__ __device__ constexpr int lt_floats(int P) { return P > 0 ? 256 * P + 288 : 0; }
 
 // Sticky device status shared by every kernel of a context.
-struct DevStatus {
+struct __align__(16) DevStatus {
   int error;          // 0 = ok; >0 = capacity overflow (see need); <0 = fatal
   int fail_slice;     // slice index at which the first error was raised
   int need_cap;       // particles a tile must hold
@@ -101,6 +101,22 @@ __device__ __forceinline__ bool pass_skipped(const DevStatus* st, int pass) {
   if (pass <= 1) return false;
   const int done = st->pass_done;
   return done > 0 && done < pass;
+}
+
+// The words of the device status a slice kernel checks before its work, read
+// with two 16-byte loads (error .. need_inbox, cursor .. beam_drops) that a
+// kernel issues together with its first data loads.
+struct StatusSnap {
+  int error, cursor, pass_done;
+};
+__device__ __forceinline__ StatusSnap status_snap(const DevStatus* st) {
+  const int4* p = reinterpret_cast<const int4*>(st);
+  const int4 a = p[0], b = p[1];
+  return StatusSnap{a.x, b.x, b.y};
+}
+// pass_skipped on a snapshot
+__device__ __forceinline__ bool snap_skipped(const StatusSnap& s, int pass) {
+  return pass > 1 && s.pass_done > 0 && s.pass_done < pass;
 }
 
 enum { QP_OK = 0, QP_OVERFLOW = 1 };

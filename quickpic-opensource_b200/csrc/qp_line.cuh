@@ -222,18 +222,21 @@ __device__ __forceinline__ float2 shfl2(float2 v, int src) {
 //   x[j] = in_scale * (in[j] + in2[j]),  j = 0..n   (in2 may be null)
 // written to out[0..n] (shared memory, 16-byte aligned; may alias `in`).
 // `in` and `in2` may point to global or shared memory, 8-byte aligned.
+// The line of a register transform held by one lane: x[2m], x[2m+1] for
+// m = lane + 32 a (a = 0..P-1) and, on lane 0, x[n].
 template <int P>
-__device__ __forceinline__ void reg_line(const float* in, const float* in2, float in_scale,
-                                         float* out, int parity, const float* T, int lane) {
-  // T: the lane table of this line length staged in shared memory (lt_* layout)
-  const float2* tw3 = reinterpret_cast<const float2*>(T + lt_tw3(P));
-  const float2* tw4 = reinterpret_cast<const float2*>(T + lt_tw4(P));
-  const float2* tw5 = reinterpret_cast<const float2*>(T + lt_tw5(P));
-  const float2* uwl = reinterpret_cast<const float2*>(T + lt_uw(P));
-  constexpr int N = 64 * P;
-  const unsigned FULL = 0xffffffffu;
-  // 1. the line: x[2m], x[2m+1] for m = lane + 32 a, and x[n]
+struct LineRegs {
   float2 xp[P];
+  float xn;
+};
+
+// 1. the line x = in_scale * (in + in2) into the lanes' registers.  A kernel
+//    may issue this before it reads the device status, so that both loads
+//    wait for L2 together.
+template <int P>
+__device__ __forceinline__ void reg_line_load(const float* in, const float* in2, float in_scale,
+                                              LineRegs<P>& r, int lane) {
+  constexpr int N = 64 * P;
 #pragma unroll
   for (int a = 0; a < P; ++a) {
     const int m = lane + 32 * a;
@@ -243,14 +246,30 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
       v.x += w.x;
       v.y += w.y;
     }
-    xp[a] = make_float2(v.x * in_scale, v.y * in_scale);
+    r.xp[a] = make_float2(v.x * in_scale, v.y * in_scale);
   }
-  float xn = 0.f;
+  r.xn = 0.f;
   if (lane == 0) {
-    xn = in[N];
+    float xn = in[N];
     if (in2) xn += in2[N];
-    xn *= in_scale;
+    r.xn = xn * in_scale;
   }
+}
+
+// 2-8. the transform of a loaded line, written to out[0..n] (shared memory,
+//      16-byte aligned; may alias the line's source)
+template <int P>
+__device__ __forceinline__ void reg_line_core(const LineRegs<P>& r, float* out, int parity,
+                                              const float* T, int lane) {
+  // T: the lane table of this line length staged in shared memory (lt_* layout)
+  const float2* tw3 = reinterpret_cast<const float2*>(T + lt_tw3(P));
+  const float2* tw4 = reinterpret_cast<const float2*>(T + lt_tw4(P));
+  const float2* tw5 = reinterpret_cast<const float2*>(T + lt_tw5(P));
+  const float2* uwl = reinterpret_cast<const float2*>(T + lt_uw(P));
+  constexpr int N = 64 * P;
+  const unsigned FULL = 0xffffffffu;
+  const float2* xp = r.xp;
+  const float xn = r.xn;
   __syncwarp();
   float sigma = 0.f;
   if (parity) {
@@ -387,6 +406,14 @@ __device__ __forceinline__ void reg_line(const float* in, const float* in2, floa
   }
   if (lane == 0) out[N] = parity ? 2.f * yh : 0.f;
   __syncwarp();
+}
+
+template <int P>
+__device__ __forceinline__ void reg_line(const float* in, const float* in2, float in_scale,
+                                         float* out, int parity, const float* T, int lane) {
+  LineRegs<P> r;
+  reg_line_load<P>(in, in2, in_scale, r, lane);
+  reg_line_core<P>(r, out, parity, T, lane);
 }
 
 // Per-warp line transform of x = in_scale * (in + in2) into the shared line

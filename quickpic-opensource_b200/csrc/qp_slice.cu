@@ -47,7 +47,12 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   float* T = smem + (P > 0 ? 8 : 16) * pitch;
   if (P > 0) stage_lane_table(T, ty);  // constant tables: staged before the wait
   grid_dep_sync();
-  if (st->error) return;
+  // the columns of qe and qb are read with the status: one L2 round trip
+  LineRegs<(P > 0 ? P : 1)> r;
+  if (P > 0 && (warp == 0 || (warp == 1 && a.qb)))
+    reg_line_load<(P > 0 ? P : 1)>((warp == 0 ? a.qe : a.qb) + co, nullptr, a.norm, r, lane);
+  const StatusSnap sn = status_snap(st);
+  if (sn.error) return;
   // a new slice: no pass of it has converged yet (the passes follow this kernel)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     DevStatus* ws = const_cast<DevStatus*>(st);
@@ -56,13 +61,14 @@ __global__ void __launch_bounds__(256) k_slice_a(SliceA a, GridDims g, KCoef K, 
   }
   if (P > 0) __syncthreads();
   // phase 1: forward y of qe (warp 0) and qb (warp 1)
-  if (warp == 0) {
-    line_transform<P>(a.qe + co, nullptr, a.norm, L, S, g.indy, 0, ty, T, lane);
-  } else if (warp == 1) {
-    if (a.qb)
-      line_transform<P>(a.qb + co, nullptr, a.norm, L, S, g.indy, 0, ty, T, lane);
+  if (warp == 0 || (warp == 1 && a.qb)) {
+    if constexpr (P > 0)
+      reg_line_core<P>(r, L, 0, T, lane);
     else
-      for (int j = lane; j <= n; j += 32) L[j] = 0.f;
+      line_transform<P>((warp == 0 ? a.qe : a.qb) + co, nullptr, a.norm, L, S, g.indy, 0, ty, T,
+                        lane);
+  } else if (warp == 1) {
+    for (int j = lane; j <= n; j += 32) L[j] = 0.f;
   }
   __syncthreads();
   // phase 2: the solves of the slice start, mode by mode
@@ -201,15 +207,27 @@ __global__ void __launch_bounds__(288) k_slice_b(SliceB b, GridDims g, KCoef K, 
       b.vpot_out[2][o] = az;
     }
   }
-  // relative change of B_perp for the convergence-controlled iteration
+  // relative change of B_perp for the convergence-controlled iteration: the
+  // CTA's sums are formed in shared memory and added with one reduction each
+  // (every CTA's reductions go to the same two words, and a reduction per
+  // warp made those words an L2 bottleneck)
+  __shared__ float rsum[2][9];
   r_num = warp_sum(r_num);
   r_den = warp_sum(r_den);
-  if (lane == 0 && b.track_residual) {
-    atomicAdd(&st->resid_num, r_num);
-    atomicAdd(&st->resid_den, r_den);
+  if (lane == 0) {
+    rsum[0][warp] = r_num;
+    rsum[1][warp] = r_den;
   }
   __syncthreads();
   if (b.track_residual && threadIdx.x == 0) {
+    float sn = 0.f, sd = 0.f;
+#pragma unroll
+    for (int w = 0; w < 9; ++w) {
+      sn += rsum[0][w];
+      sd += rsum[1][w];
+    }
+    atomicAdd(&st->resid_num, sn);
+    atomicAdd(&st->resid_den, sd);
     // the last CTA to finish has the complete sums: decide, and reset them for
     // the next pass (which starts only after this kernel)
     __threadfence();

@@ -115,3 +115,36 @@ def test_graph_signature_follows_buffer_swaps(qp):
         _close(sim, bm, sp, c)
     for k in out[0]:
         assert rel_l2(out[0][k], out[1][k]) < 1e-4, k
+
+
+@pytest.mark.parametrize("use_graphs", [False, True], ids=["direct", "graph"])
+def test_pass_loop_stops_at_iter(qp, use_graphs):
+    """A tolerance no slice meets (1e-12) with at most 5 passes: every slice
+    stops after 5 passes or earlier on the stall rule (which needs 8), so
+    each of the 32 slices takes exactly 5 and all are counted unconverged."""
+    cfg = make_config(ind=(6, 6, 5), iter=5)
+    cfg["tol"] = 1e-12
+    c, sp, bm, sim = _sim(qp, cfg, use_graphs)
+    st = sim.step3d()
+    assert st.iterations == 5 * 32, st.iterations
+    assert st.unconverged == 32
+    _close(sim, bm, sp, c)
+
+
+def test_graph_pass_counts_match_direct(qp):
+    """Graph replay runs the passes the direct launches run: per-step pass
+    totals agree (within FP32 roundoff of the residual near the tolerance)
+    on two 128^2 x 128 steps, the second capped from the first's record."""
+    cfg = make_config(ind=(7, 7, 7), iter=16)
+    cfg["tol"] = 1e-4
+    res = []
+    for graphs in (True, False):
+        c, sp, bm, sim = _sim(qp, cfg, graphs, dt=10.0)
+        st = [sim.step3d() for _ in range(2)]
+        res.append(([x.iterations for x in st], [x.unconverged for x in st],
+                    sim.get_3d("bexyz")))
+        _close(sim, bm, sp, c)
+    (ig, ug, bg), (idir, ud, bd) = res
+    for a, b in zip(ig, idir):
+        assert abs(a - b) <= 0.02 * b, (ig, idir)
+    assert rel_l2(bg, bd) < 1e-4
