@@ -63,7 +63,12 @@ __host__ __device__ constexpr int lt_tw4(int P) { return 128 * P; }   // float2 
 __host__ __device__ constexpr int lt_uw(int P) { return 192 * P; }    // float2 [P][32]
 __host__ __device__ constexpr int lt_tw5(int P) { return 256 * P; }   // float2 [4][32]
 __host__ __device__ constexpr int lt_tw3(int P) { return 256 * P + 256; }  // float2 [16]
-__host__ __device__ constexpr int lt_floats(int P) { return P > 0 ? 256 * P + 288 : 0; }
+__host__ __device__ constexpr int lt_w32(int P) { return 256 * P + 288; }  // float2 [4][8]
+__host__ __device__ constexpr int lt_floats(int P) { return P > 0 ? 256 * P + 352 : 0; }
+// Lines of 64 P points whose 32-point lane stage goes through shared memory
+// (reg_line_tail_xs) instead of shuffles; their unscramble table is in lane
+// order, the others' in bit-reversed lane order.
+__host__ __device__ constexpr bool line_xs(int P) { return P == 8; }
 
 // Sticky device status shared by every kernel of a context.
 struct __align__(16) DevStatus {

@@ -54,7 +54,7 @@ int line_tables_build(LineTablesHost* t, int logn) {
     for (int k2 = 0; k2 < P; ++k2)
       for (int l = 0; l < 32; ++l) {
         f2(lt_tw4(P), 32 * k2 + l, tw[l * k2]);
-        f2(lt_uw(P), 32 * k2 + l, uw[k2 + P * brev5(l)]);
+        f2(lt_uw(P), 32 * k2 + l, uw[k2 + P * (line_xs(P) ? l : brev5(l))]);
       }
     for (int si = 0; si < 4; ++si) {
       const int st = 16 >> si;
@@ -63,6 +63,9 @@ int line_tables_build(LineTablesHost* t, int logn) {
            (l & st) ? tw[(l & (st - 1)) * (16 / st) * P] : make_float2(1.f, 0.f));
     }
     for (int k = 0; k < 16; ++k) f2(lt_tw3(P), k, tw[k * P]);
+    // exp(-2 pi i q c / 32) = tw[q c P] for the exchange form's 8 x 4 split
+    for (int q = 0; q < 4; ++q)
+      for (int c = 0; c < 8; ++c) f2(lt_w32(P), 8 * q + c, tw[q * c * P]);
   }
   size_t bytes = sizeof(float) * 2 * (n + 1) + sizeof(float2) * (2 * h + 1) + 64 +
                  sizeof(float) * lt.size() + 16;

@@ -256,6 +256,158 @@ __device__ __forceinline__ void reg_line_load(const float* in, const float* in2,
   }
 }
 
+// In-place 8-point DFT, natural order in and out (radix 2 x 4: the even
+// outputs are the 4-point DFT of x[m] + x[m+4], the odd ones that of
+// (x[m] - x[m+4]) exp(-2 pi i m / 8)).
+__device__ __forceinline__ void dft8(float2 (&x)[8]) {
+  const float r = 0.70710678118654752f;  // cos(pi / 4)
+  const float2 a0 = make_float2(x[0].x + x[4].x, x[0].y + x[4].y);
+  const float2 a1 = make_float2(x[0].x - x[4].x, x[0].y - x[4].y);
+  const float2 b0 = make_float2(x[2].x + x[6].x, x[2].y + x[6].y);
+  const float2 b1 = make_float2(x[2].x - x[6].x, x[2].y - x[6].y);
+  const float2 c0 = make_float2(x[1].x + x[5].x, x[1].y + x[5].y);
+  const float2 c1 = make_float2(x[1].x - x[5].x, x[1].y - x[5].y);
+  const float2 d0 = make_float2(x[3].x + x[7].x, x[3].y + x[7].y);
+  const float2 d1 = make_float2(x[3].x - x[7].x, x[3].y - x[7].y);
+  // even outputs
+  const float2 e0 = make_float2(a0.x + b0.x, a0.y + b0.y);
+  const float2 e1 = make_float2(a0.x - b0.x, a0.y - b0.y);
+  const float2 g0 = make_float2(c0.x + d0.x, c0.y + d0.y);
+  const float2 g1 = make_float2(c0.x - d0.x, c0.y - d0.y);
+  // odd outputs: b1 (-i), c1 exp(-i pi/4), d1 exp(-3 i pi/4)
+  const float2 bb = make_float2(b1.y, -b1.x);
+  const float2 cc = make_float2(r * (c1.x + c1.y), r * (c1.y - c1.x));
+  const float2 dd = make_float2(r * (d1.y - d1.x), -r * (d1.x + d1.y));
+  const float2 h0 = make_float2(a1.x + bb.x, a1.y + bb.y);
+  const float2 h1 = make_float2(a1.x - bb.x, a1.y - bb.y);
+  const float2 k0 = make_float2(cc.x + dd.x, cc.y + dd.y);
+  const float2 k1 = make_float2(cc.x - dd.x, cc.y - dd.y);
+  x[0] = make_float2(e0.x + g0.x, e0.y + g0.y);
+  x[4] = make_float2(e0.x - g0.x, e0.y - g0.y);
+  x[2] = make_float2(e1.x + g1.y, e1.y - g1.x);  // e1 - i g1
+  x[6] = make_float2(e1.x - g1.y, e1.y + g1.x);  // e1 + i g1
+  x[1] = make_float2(h0.x + k0.x, h0.y + k0.y);
+  x[5] = make_float2(h0.x - k0.x, h0.y - k0.y);
+  x[3] = make_float2(h1.x + k1.y, h1.y - k1.x);  // h1 - i k1
+  x[7] = make_float2(h1.x - k1.y, h1.y + k1.x);  // h1 + i k1
+}
+
+// Steps 5-8 of the register transform for P = 8 (256-point complex FFT,
+// 8 values per lane), through shared memory instead of 5 shuffle stages.
+// In: w[k2] = f_k2(lane), the input of the 32-point DFT over the lanes.
+// 5. The 32-point DFT as 8 x 4 (lane l = q + 4 b): the values move through
+//    `out` so that lane t = 4 r + q holds f_r(q + 4 b), b = 0..7 (rows XOR-
+//    swizzled by 4 (r & 3): the stores and the strided loads hit distinct
+//    banks); an 8-point DFT over b, the twiddle exp(-2 pi i q c / 32), and a
+//    4-point DFT over q across the four lanes of r (two shuffle stages) leave
+//    Z[r + 8 (c + 8 brev2(q))] in register c.
+// 6. Z goes back through `out` (swizzled by block) so that lane l holds its
+//    block Z[8 l + k2] and the partners Z[256 - 8 l - k2] of the unscramble.
+// 7-8. Unscramble, prefix sum and the output as in the shuffle form, with
+//    the blocks in lane order.
+template <int P>
+__device__ __forceinline__ void reg_line_tail_xs(float2 (&w)[P], float* out, int parity,
+                                                 float sigma, const float* T, const float2* uwl,
+                                                 int lane) {
+  static_assert(P == 8, "the exchange form is written for 512-point lines");
+  constexpr int N = 64 * P;
+  const unsigned FULL = 0xffffffffu;
+  float2* X = reinterpret_cast<float2*>(out);  // 32 P float2 = N floats
+#pragma unroll
+  for (int k2 = 0; k2 < P; ++k2) X[32 * k2 + (lane ^ (4 * (k2 & 3)))] = w[k2];
+  __syncwarp();
+  const int r = lane >> 2, q = lane & 3;
+  float2 f[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) f[b] = X[32 * r + ((q + 4 * b) ^ (4 * (r & 3)))];
+  dft8(f);
+  const float2* w32 = reinterpret_cast<const float2*>(T + lt_w32(P)) + 8 * q;
+#pragma unroll
+  for (int c = 1; c < 8; ++c) f[c] = cmul(f[c], w32[c]);
+  {
+    // radix-2 DIF over q: lanes with bit 2 of q keep (p - v), times -i on q = 3
+    const float sg = (q & 2) ? -1.f : 1.f;
+    const bool rot = q == 3;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const float2 p = shfl_xor2(f[c], 2);
+      const float2 d = make_float2(fmaf(sg, f[c].x, p.x), fmaf(sg, f[c].y, p.y));
+      f[c] = rot ? make_float2(d.y, -d.x) : d;
+    }
+    const float sg1 = (q & 1) ? -1.f : 1.f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const float2 p = shfl_xor2(f[c], 1);
+      f[c] = make_float2(fmaf(sg1, f[c].x, p.x), fmaf(sg1, f[c].y, p.y));
+    }
+  }
+  __syncwarp();  // every lane has read its exchange values before Z overwrites them
+  const int qb = ((q & 1) << 1) | (q >> 1);  // brev2(q)
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int kap = c + 8 * qb;  // the block of this value
+    X[8 * kap + (r ^ ((kap >> 1) & 7))] = f[c];
+  }
+  __syncwarp();
+  float2 A[8], B[8];
+  {
+    const int sw = (lane >> 1) & 7;
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) A[k2] = X[8 * lane + (k2 ^ sw)];
+    const int lp = 31 - lane, swp = (lp >> 1) & 7;
+#pragma unroll
+    for (int k2 = 1; k2 < 8; ++k2) B[k2] = X[8 * lp + ((8 - k2) ^ swp)];
+    const int l0 = (32 - lane) & 31;
+    B[0] = X[8 * l0 + ((l0 >> 1) & 7)];
+  }
+  float ev[P], od[P];
+  float yh = 0.f;
+  float run = 0.f;
+#pragma unroll
+  for (int k2 = 0; k2 < P; ++k2) {
+    const int k = k2 + P * lane;
+    const float2 a = A[k2];
+    const float2 b = make_float2(B[k2].x, -B[k2].y);
+    float2 Y;
+    if (k == 0) {
+      Y = make_float2(a.x + a.y, 0.f);
+      yh = a.x - a.y;
+    } else {
+      const float2 E = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
+      const float2 D = make_float2(a.x - b.x, a.y - b.y);
+      const float2 u = cmul(uwl[32 * k2 + lane], D);
+      Y = make_float2(E.x + 0.5f * u.y, E.y - 0.5f * u.x);
+    }
+    float term;
+    if (parity == 0) {
+      ev[k2] = (k == 0) ? 0.f : -2.f * Y.y;
+      term = (k == 0) ? Y.x : 2.f * Y.x;
+    } else {
+      ev[k2] = 2.f * Y.x;
+      term = (k == 0) ? 0.f : -2.f * Y.y;
+    }
+    run += term;
+    od[k2] = run;
+  }
+  // exclusive scan of the block sums, blocks in lane order
+  float inc = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float u = __shfl_up_sync(FULL, inc, o);
+    if (lane >= o) inc += u;
+  }
+  float base = inc - run;
+  if (parity) base += 2.f * sigma;
+  __syncwarp();  // every lane has read Z before the line overwrites it
+  float* o = out + 2 * P * lane;
+#pragma unroll
+  for (int k2 = 0; k2 < P; k2 += 2)
+    *reinterpret_cast<float4*>(o + 2 * k2) =
+        make_float4(ev[k2], base + od[k2], ev[k2 + 1], base + od[k2 + 1]);
+  if (lane == 0) out[N] = parity ? 2.f * yh : 0.f;
+  __syncwarp();
+}
+
 // 2-8. the transform of a loaded line, written to out[0..n] (shared memory,
 //      16-byte aligned; may alias the line's source)
 template <int P>
@@ -329,83 +481,88 @@ __device__ __forceinline__ void reg_line_core(const LineRegs<P>& r, float* out, 
   // 4. twiddle exp(-2 pi i lane k2 / (n/2))
 #pragma unroll
   for (int k2 = 1; k2 < P; ++k2) w[k2] = cmul(w[k2], tw4[32 * k2 + lane]);
-  // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles): the lower
-  //    lane of a pair keeps v + p, the upper one (p - v) * twiddle; written as
-  //    fma(sign, v, p) times a twiddle that is 1 on the lower lanes (and on
-  //    every lane in the last stage)
-#pragma unroll
-  for (int s = 16; s >= 1; s >>= 1) {
-    const bool hi = (lane & s) != 0;
-    const float sg = hi ? -1.f : 1.f;
-    // the table holds (1, 0) for the lower lanes of each stage
-    const int si = (s == 16) ? 0 : (s == 8) ? 1 : (s == 4) ? 2 : 3;
-    const float2 tws = (s > 1) ? tw5[32 * si + lane] : make_float2(1.f, 0.f);
-#pragma unroll
-    for (int k2 = 0; k2 < P; ++k2) {
-      const float2 v = w[k2];
-      const float2 p = shfl_xor2(v, s);
-      const float2 d = make_float2(fmaf(sg, v.x, p.x), fmaf(sg, v.y, p.y));
-      w[k2] = (s > 1) ? cmul(d, tws) : d;
-    }
-  }
-  // 6. real-FFT unscramble: Y[k] = sum_j y[j] exp(-2 pi i j k / n), k = k2 + P k1
-  const int k1 = brev5(lane);
-  const int src0 = brev5((32 - k1) & 31);
-  float ev[P], od[P];
-  float yh = 0.f;
-  float run = 0.f;
-#pragma unroll
-  for (int k2 = 0; k2 < P; ++k2) {
-    float2 B = (k2 == 0) ? shfl2(w[0], src0) : shfl_xor2(w[(P - k2) % P], 31);
-    B.y = -B.y;
-    const int k = k2 + P * k1;
-    const float2 A = w[k2];
-    float2 Y;
-    if (k == 0) {
-      Y = make_float2(A.x + A.y, 0.f);
-      yh = A.x - A.y;
-    } else {
-      const float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y + B.y));
-      const float2 D = make_float2(A.x - B.x, A.y - B.y);
-      const float2 q = cmul(uwl[32 * k2 + lane], D);
-      Y = make_float2(E.x + 0.5f * q.y, E.y - 0.5f * q.x);
-    }
-    // sine:   out[2k] = -2 Im Y[k], out[2k+1] = Re Y[0] + 2 sum_{m=1..k} Re Y[m]
-    // cosine: out[2k] =  2 Re Y[k], out[2k+1] = 2 sigma - 2 sum_{m=1..k} Im Y[m]
-    float term;
-    if (parity == 0) {
-      ev[k2] = (k == 0) ? 0.f : -2.f * Y.y;
-      term = (k == 0) ? Y.x : 2.f * Y.x;
-    } else {
-      ev[k2] = 2.f * Y.x;
-      term = (k == 0) ? 0.f : -2.f * Y.y;
-    }
-    run += term;
-    od[k2] = run;
-  }
-  // 7. exclusive scan of the block sums in block order k1
-  const float blk = __shfl_sync(FULL, run, k1);  // lane l: sum of block l
-  float inc = blk;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const float u = __shfl_up_sync(FULL, inc, o);
-    if (lane >= o) inc += u;
-  }
-  float base = __shfl_sync(FULL, inc - blk, k1);
-  if (parity) base += 2.f * sigma;
-  __syncwarp();
-  // 8. out[2k], out[2k+1] for the lane's block k = P k1 .. P k1 + P - 1
-  float* o = out + 2 * P * k1;
-  if (P == 1) {
-    *reinterpret_cast<float2*>(o) = make_float2(ev[0], base + od[0]);
+  if constexpr (line_xs(P)) {
+    reg_line_tail_xs<P>(w, out, parity, sigma, T, uwl, lane);
+    return;
   } else {
-#pragma unroll
-    for (int k2 = 0; k2 < P; k2 += 2)
-      *reinterpret_cast<float4*>(o + 2 * k2) =
-          make_float4(ev[k2], base + od[k2], ev[(k2 + 1) % P], base + od[(k2 + 1) % P]);
+    // 5. 32-point DFT across the lanes (radix-2 DIF with shuffles): the lower
+    //    lane of a pair keeps v + p, the upper one (p - v) * twiddle; written as
+    //    fma(sign, v, p) times a twiddle that is 1 on the lower lanes (and on
+    //    every lane in the last stage)
+  #pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+      const bool hi = (lane & s) != 0;
+      const float sg = hi ? -1.f : 1.f;
+      // the table holds (1, 0) for the lower lanes of each stage
+      const int si = (s == 16) ? 0 : (s == 8) ? 1 : (s == 4) ? 2 : 3;
+      const float2 tws = (s > 1) ? tw5[32 * si + lane] : make_float2(1.f, 0.f);
+  #pragma unroll
+      for (int k2 = 0; k2 < P; ++k2) {
+        const float2 v = w[k2];
+        const float2 p = shfl_xor2(v, s);
+        const float2 d = make_float2(fmaf(sg, v.x, p.x), fmaf(sg, v.y, p.y));
+        w[k2] = (s > 1) ? cmul(d, tws) : d;
+      }
+    }
+    // 6. real-FFT unscramble: Y[k] = sum_j y[j] exp(-2 pi i j k / n), k = k2 + P k1
+    const int k1 = brev5(lane);
+    const int src0 = brev5((32 - k1) & 31);
+    float ev[P], od[P];
+    float yh = 0.f;
+    float run = 0.f;
+  #pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+      float2 B = (k2 == 0) ? shfl2(w[0], src0) : shfl_xor2(w[(P - k2) % P], 31);
+      B.y = -B.y;
+      const int k = k2 + P * k1;
+      const float2 A = w[k2];
+      float2 Y;
+      if (k == 0) {
+        Y = make_float2(A.x + A.y, 0.f);
+        yh = A.x - A.y;
+      } else {
+        const float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y + B.y));
+        const float2 D = make_float2(A.x - B.x, A.y - B.y);
+        const float2 q = cmul(uwl[32 * k2 + lane], D);
+        Y = make_float2(E.x + 0.5f * q.y, E.y - 0.5f * q.x);
+      }
+      // sine:   out[2k] = -2 Im Y[k], out[2k+1] = Re Y[0] + 2 sum_{m=1..k} Re Y[m]
+      // cosine: out[2k] =  2 Re Y[k], out[2k+1] = 2 sigma - 2 sum_{m=1..k} Im Y[m]
+      float term;
+      if (parity == 0) {
+        ev[k2] = (k == 0) ? 0.f : -2.f * Y.y;
+        term = (k == 0) ? Y.x : 2.f * Y.x;
+      } else {
+        ev[k2] = 2.f * Y.x;
+        term = (k == 0) ? 0.f : -2.f * Y.y;
+      }
+      run += term;
+      od[k2] = run;
+    }
+    // 7. exclusive scan of the block sums in block order k1
+    const float blk = __shfl_sync(FULL, run, k1);  // lane l: sum of block l
+    float inc = blk;
+  #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float u = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += u;
+    }
+    float base = __shfl_sync(FULL, inc - blk, k1);
+    if (parity) base += 2.f * sigma;
+    __syncwarp();
+    // 8. out[2k], out[2k+1] for the lane's block k = P k1 .. P k1 + P - 1
+    float* o = out + 2 * P * k1;
+    if (P == 1) {
+      *reinterpret_cast<float2*>(o) = make_float2(ev[0], base + od[0]);
+    } else {
+  #pragma unroll
+      for (int k2 = 0; k2 < P; k2 += 2)
+        *reinterpret_cast<float4*>(o + 2 * k2) =
+            make_float4(ev[k2], base + od[k2], ev[(k2 + 1) % P], base + od[(k2 + 1) % P]);
+    }
+    if (lane == 0) out[N] = parity ? 2.f * yh : 0.f;
+    __syncwarp();
   }
-  if (lane == 0) out[N] = parity ? 2.f * yh : 0.f;
-  __syncwarp();
 }
 
 template <int P>
