@@ -333,8 +333,7 @@ int qp_beam_read_restart(qp_beam* b, const char* dir, int beam, int rank, int st
  * every slice with the same two (a replay first checks every pointer and
  * value the graph holds against the current ones and captures again when a
  * buffer was grown or replaced); the results are the same as with direct
- * launches; ignored with predict = 3, while recording, and in checked mode
- * (QP_SYNC_CHECK=1);
+ * launches; ignored while recording and in checked mode (QP_SYNC_CHECK=1);
  * dt = the 3D time step (simulation.dt): dt > 0 (with store3d = 1) ends the
  * step with beam3d%push of every beam with the stored bexyz, bbxyz
  * (simulation_class.f03:753-757), dt = 0 leaves the beams where they are. */

@@ -82,13 +82,15 @@ def test_loss_gradient_matches_oracle(qp, N):
     net.close()
 
 
-def _sim(qp, ind, peak, sigma_r, tol=1e-4, iter=16, predict=0, seed_center=2.5):
+def _sim(qp, ind, peak, sigma_r, tol=1e-4, iter=16, predict=0, seed_center=2.5,
+         use_graphs=False):
     c = qp.Context(ind[0], ind[1], ind[2], BOX)
     sp = qp.Species2d(c, ppc=(2, 2))
     bm = qp.Beam3d(c, [64, 64, 64], q=-1.0, m=1.0, gamma=20000.0, peak_density=peak,
                    quiet_start=True, center=[0.0, 0.0, seed_center],
                    sigma=[sigma_r, sigma_r, 0.5], sigma_v=[0.0, 0.0, 0.0])
-    sim = qp.Simulation(c, [sp], [bm], iter=iter, store3d=True, tol=tol, predict=predict)
+    sim = qp.Simulation(c, [sp], [bm], iter=iter, store3d=True, tol=tol, predict=predict,
+                        use_graphs=use_graphs)
     return c, sp, bm, sim
 
 
@@ -146,4 +148,14 @@ def test_learned_start_needs_fewer_passes(qp):
     assert res[3][0] < res[0][0]
     for k in (2, 3):
         assert rel_l2(res[3][k], res[0][k]) < 1e-3
+    # the learned start replayed from CUDA graphs (the network's launches
+    # captured with the slice) gives the same passes and fields
+    c, sp, bm, sim = _sim(qp, (7, 7, 7), 4.0, 0.3, predict=3, use_graphs=True)
+    sim.set_predictor(net)
+    s = sim.step3d()
+    assert sim.graph_captures >= 2
+    assert abs(s.iterations - res[3][0]) <= 0.02 * res[3][0], (s.iterations, res[3][0])
+    for k, name in ((2, "bexyz"), (3, "bbxyz")):
+        assert rel_l2(sim.get_3d(name), res[3][k]) < 1e-3
+    _close(sim, bm, sp, c)
     _close(net, data)
