@@ -75,18 +75,11 @@ __device__ __forceinline__ void deposit_q(float* q, const TileGeom& tg, int noff
 // Charge deposit with the run scheme of k_amjdp: 4 consecutive particles per
 // thread, corner weights of a run of particles in one cell summed in
 // registers, then added to q (which must be zero on entry) by deposit_q.
-__global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, float* q,
-                                                     DevStatus* st) {
-  grid_dep_sync();
-  if (st && st->error) return;
-  const int t = blockIdx.x;
+// The n particles of tile t (all the CTA's threads take part).
+__device__ __forceinline__ void deposit_tile(const PartBuf& P, const TileGeom& tg, int t, int n,
+                                             float* q, DevStatus* st) {
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
-  const int n = P.count[t];
-  if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
-    if (threadIdx.x == 0) raise_error(st, -6);
-    return;
-  }
   const long long base = (long long)t * P.cap;
   for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * blockDim.x) {
     const float4 X = *reinterpret_cast<const float4*>(P.c[0] + base + k0);
@@ -129,6 +122,19 @@ __global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, flo
     }
     if (cell >= 0) deposit_q(q, tg, noffp, moffp, cell, acc);
   }
+}
+
+__global__ void __launch_bounds__(256) k_deposit_rho(PartBuf P, TileGeom tg, float* q,
+                                                     DevStatus* st) {
+  grid_dep_sync();
+  if (st && st->error) return;
+  const int t = blockIdx.x;
+  const int n = P.count[t];
+  if (n < 0 || n > P.cap) {  // a count beyond the tile's slots: never read past them
+    if (threadIdx.x == 0) raise_error(st, -6);
+    return;
+  }
+  deposit_tile(P, tg, t, n, q, st);
 }
 
 __global__ void __launch_bounds__(256) k_extpsi(PartBuf P, TileGeom tg, const float* psi,
@@ -470,6 +476,16 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
   int noffp, moffp;
   tile_origin(tg, t, &noffp, &moffp);
   const int n = A.count[t];  // read with the field planes: the waits overlap
+  if (f.zero_q) {
+    // the tile's 16 x 16 nodes of the charge plane, and on the last tile
+    // column / row the rest of the row pitch / the guard row: every node of
+    // the plane is cleared by exactly one tile
+    const int x1 = (noffp + TILE >= tg.nx) ? tg.rp : noffp + TILE;
+    const int y1 = (moffp + TILE >= tg.ny) ? tg.ny + 1 : moffp + TILE;
+    const int w = x1 - noffp, h = y1 - moffp;
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x)
+      f.zero_q[(long long)(moffp + i / w) * tg.rp + noffp + i % w] = 0.f;
+  }
   if (MODE != 2) {
     const float* const planes[6] = {f.fx, f.fy, f.bx, f.by, f.bz, f.psit};
     stage_planes<6>(sf, planes, 6, tg, noffp, moffp);
@@ -715,7 +731,7 @@ __global__ void __launch_bounds__(256) k_push(PartBuf A, PartBuf B, Inbox ib, Ti
 // the particle order does not depend on the order in which the atomics of the
 // push handed out inbox slots.
 __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg, int p2max,
-                                                DevStatus* st) {
+                                                DevStatus* st, float* dq) {
   grid_dep_sync();
   extern __shared__ unsigned long long skey[];
   int* sidx = reinterpret_cast<int*>(skey + p2max);
@@ -784,6 +800,9 @@ __global__ void __launch_bounds__(256) k_insert(PartBuf B, Inbox ib, TileGeom tg
     B.count[t] = stay + nin;
     ib.count[t] = 0;
   }
+  // the next slice's charge: every particle of the re-binned tile (the
+  // movers were written above; the barrier makes them visible to the CTA)
+  if (dq) deposit_tile(B, tg, t, stay + nin, dq, st);
 }
 
 }  // namespace
@@ -797,11 +816,11 @@ int part_kernels_init() {
 }
 
 void launch_insert(const PartBuf& B, const Inbox& ib, const TileGeom& tg, DevStatus* st,
-                   cudaStream_t s) {
+                   cudaStream_t s, float* deposit_q) {
   int p2 = 1;
   while (p2 < ib.cap) p2 <<= 1;
   const size_t smem = (size_t)p2 * (sizeof(unsigned long long) + sizeof(int));
-  launch_pdl(k_insert, tg.ntiles, 256, smem, s, B, ib, tg, p2, st);
+  launch_pdl(k_insert, tg.ntiles, 256, smem, s, B, ib, tg, p2, st, deposit_q);
 }
 
 void launch_deposit_rho(const PartBuf& P, const TileGeom& tg, float* q, const DevStatus* st,

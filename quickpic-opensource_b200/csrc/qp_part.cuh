@@ -41,6 +41,8 @@ struct GatherPlanes {
   int combine;       // 1: the push uses -fxy + (by, -bx), the final slice force
   const float* psi;  // amjdp only, optional: form p6, p7 from psi first (extpsi)
   int pass;          // amjdp only: predictor-corrector pass (pass_skipped), 0 = none
+  float* zero_q;     // push only, optional: clear the charge-plane nodes this tile
+                     // owns (k_insert then deposits the next slice's charge)
 };
 
 int part_kernels_init();
@@ -58,7 +60,9 @@ void launch_amjdp(const PartBuf& P, const TileGeom& tg, const GatherPlanes& f, f
 void launch_push(int mode, const PartBuf& A, const PartBuf& B, const Inbox& ib,
                  const TileGeom& tg, const GatherPlanes& f, float qbm, float dt, float dex,
                  DevStatus* st, cudaStream_t s);
+// deposit_q (optional): after the re-bin, deposit the charge of every
+// particle of the tile into deposit_q (zero on entry), as k_deposit_rho does
 void launch_insert(const PartBuf& B, const Inbox& ib, const TileGeom& tg, DevStatus* st,
-                   cudaStream_t s);
+                   cudaStream_t s, float* deposit_q = nullptr);
 
 }  // namespace qp
