@@ -199,12 +199,12 @@ int qp_species_pmove(qp_species* sp);
  * QP_PMOVE_STATIC_MIN_INBOX are rejected, and so is a step that moves more
  * particles into one tile, or fills an output tile beyond cap_out: those
  * return -1 with the sizes in qp_ctx_last_error(NULL) and leave the input
- * untouched (there is no grow-and-retry).  The first call on each device
- * looks up the array's device address, so make that call before any stream
- * capture.  Every call shares the one array: calls that overlap on the GPU
+ * untouched (there is no grow-and-retry).  Every call looks up the array's
+ * device address on the current device (so it stays valid across a
+ * cudaDeviceReset) and shares the one array: calls that overlap on the GPU
  * (other streams, other host threads) race.  The call runs on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) and returns after it
- * has synchronised that stream. */
+ * has synchronised that stream, so it cannot be captured into a CUDA graph. */
 #define QP_PMOVE_STATIC_SCRATCH_BYTES (16u << 20)
 #define QP_PMOVE_STATIC_MIN_INBOX 64
 int qp_pmove_static(int indx, int indy, const float* const* part_in, const int* count_in,
