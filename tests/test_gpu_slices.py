@@ -23,7 +23,7 @@ more than 1e-3 in it; the reasons are in each test):
   * per slice, passes to a relative change of 1e-4: <= 1e-4 against the FP64
     oracle, or 1.5x the FP32 oracle's own distance where that is larger;
   * whole 128^3 step: bexyz, bbxyz and the plasma charge q3 <= 1e-3 against
-    the FP64 oracle (the north star's full-step bar on moments).
+    the FP64 oracle (the full-step bar on moments).
 """
 import numpy as np
 import pytest
